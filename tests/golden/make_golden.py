@@ -1,0 +1,246 @@
+"""Regenerates the golden fixtures under tests/golden/ from the reference itself.
+
+Run here (where the reference checkout and its compiled binaries exist), never on the GPU
+host:   make -C oracle ref && python tests/golden/make_golden.py
+
+Outputs
+  penalties.json     MIT (mask, score) pairs and CFD position/PAM tables read from the
+                     reference's lib/otScorePenalties.cpp:3-6199, :6201-6527, :6529-6546,
+                     cross-checked against the 6,195 (mask, score) pairs embedded in the
+                     reference's legacy test index tests/data/test_genome_offTargets_indexed.issl
+  tiny_genome.issl   the reference's ISSLCreateIndex run on tests/data/test_genome_offTargets.fa
+                     with sample/slice-4-5.txt
+  case_*.npz         per case: the index inputs' digest, the queries, and the reference's
+                     outputs (ISSLScoringModule::run scores at %.17g and accept codes for every
+                     method and threshold; ISSLScoreOfftargets per-query counts and distinct
+                     site count)
+"""
+from __future__ import annotations
+
+import glob
+import hashlib
+import json
+import os
+import re
+import shutil
+import struct
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("ISSL_REFERENCE", "/root/reference")
+REF_BIN = os.path.join(REPO, "oracle", "_ref")
+sys.path.insert(0, HERE)
+sys.path.insert(0, REPO)
+
+import synth  # noqa: E402
+from cracklingplusplus_gpu_b200.slice_configs import SLICE_CONFIGS  # noqa: E402
+
+MODULE_METHODS = ["mit", "cfd", "mitAndCfd", "mitOrCfd", "avgMitCfd"]
+CLI_NAME = {"mit": "mit", "cfd": "cfd", "mitAndCfd": "and", "mitOrCfd": "or", "avgMitCfd": "avg"}
+
+
+def parse_penalties():
+    src = open(os.path.join(REF, "lib", "otScorePenalties.cpp")).read()
+    mit_block = src[src.index("precalculatedMITScores"):src.index("cfdPosPenalties")]
+    pairs = re.findall(r"\{\s*(\d+)\s*,\s*([0-9eE+.\-]+)\s*\}", mit_block)
+    mit = [(int(k), float(v)) for k, v in pairs]
+
+    def array(name, n):
+        blk = src[src.index(name):]
+        blk = blk[blk.index("{") + 1:blk.index("};")]
+        blk = re.sub(r"//[^\n]*", "", blk)
+        vals = [float(x) for x in re.findall(r"[0-9]+\.[0-9]+(?:[eE][+\-]?\d+)?|\b\d+\b", blk)]
+        assert len(vals) == n, (name, len(vals))
+        return vals
+
+    return mit, array("cfdPosPenalties[320]", 320), array("cfdPamPenalties[16]", 16)
+
+
+def legacy_mit_pairs():
+    raw = open(os.path.join(REF, "tests", "data", "test_genome_offTargets_indexed.issl"), "rb").read()
+    hdr = struct.unpack_from("<6Q", raw, 0)
+    n_pairs = hdr[5]
+    # legacy layout: a 6-word header, then the (mask, score) pairs
+    pairs = [struct.unpack_from("<Qd", raw, 48 + 16 * i) for i in range(n_pairs)]
+    return hdr, pairs
+
+
+def run(cmd, cwd=None):
+    r = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{cmd} failed: {r.stderr[-2000:]}")
+    return r
+
+
+def ref_build_index(sites, occ, masks_str, out_path, tmp):
+    """Reference ISSLCreateIndex on a sorted site text file (duplicates encode occurrences)."""
+    seqs = [synth.sig_to_seq(s) for s in sites.tolist()]
+    lines = []
+    for s, o in zip(seqs, occ.tolist()):
+        lines.extend([s] * int(o))
+    lines.sort()
+    sites_txt = os.path.join(tmp, "sites.txt")
+    with open(sites_txt, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    sc = os.path.join(tmp, "slices.txt")
+    with open(sc, "w") as f:
+        f.write("\n".join(masks_str) + "\n")
+    run([os.path.join(REF_BIN, "ISSLCreateIndex"), sites_txt, sc, "20", out_path], cwd=tmp)
+    return sorted(set(seqs))
+
+
+def ref_module(index, guides, method, threshold, tmp, optimisation="ultralow", consensus_n=0,
+               enabled=1, flags=None):
+    gp = os.path.join(tmp, "guides.tsv")
+    with open(gp, "w") as f:
+        for i, g in enumerate(guides):
+            u, c, b = flags[i] if flags else (1, 0, "?")
+            f.write(f"{g}\t{u}\t{c}\t{b}\n")
+    out = os.path.join(tmp, "module_out.tsv")
+    run([os.path.join(REF_BIN, "ref_module_driver"), index, gp, method, repr(threshold), optimisation,
+         str(consensus_n), str(enabled), out], cwd=tmp)
+    mit, cfd, codes = [], [], []
+    for line in open(out):
+        _, m, c, code = line.rstrip("\n").split("\t")
+        mit.append(float(m))
+        cfd.append(float(c))
+        codes.append(ord(code))
+    return np.array(mit), np.array(cfd), np.array(codes, np.uint8)
+
+
+def ref_cli(index, queries, method_cli, threshold, tmp):
+    qp = os.path.join(tmp, "queries.txt")
+    with open(qp, "w") as f:
+        f.write("".join(q + "\n" for q in queries))
+    work = tempfile.mkdtemp(dir=tmp)
+    r = run([os.path.join(REF_BIN, "ISSLScoreOfftargets"), index, qp, "4", repr(threshold), method_cli,
+             "cli_out.txt"], cwd=work)
+    out_files = [p for p in glob.glob(os.path.join(work, "*")) if p.endswith("cli_out.txt") and os.path.isfile(p)]
+    assert len(out_files) == 1, out_files
+    counts = []
+    for line in open(out_files[0]):
+        if line.startswith("#"):
+            continue
+        counts.append(int(line.rstrip("\n").split("\t")[3]))
+    distinct = int(re.search(r"Distinct off-targets: (\d+)", r.stderr).group(1))
+    shutil.rmtree(work)
+    return np.array(counts, np.uint64), distinct
+
+
+THRESHOLDS = [50.0, 75.0, 90.0, 99.0, 99.9]
+
+CASES = [
+    # name, seed, n_sites, n_queries, slice config, repeat fraction, planted into sites
+    ("c0_small", 11, 20000, 240, "slice-4-5", 0.05, True),
+    ("c1_small", 12, 40000, 240, "slice-8-20", 0.05, False),
+    ("c2_small", 13, 12000, 160, "slice-10-37", 0.20, False),
+    ("c4_small", 14, 30000, 160, "slice-8-28", 0.05, False),
+]
+
+
+def make_case(name, seed, n_sites, n_queries, cfg, rep, planted, tmp):
+    sites, occ, queries = synth.make_case(seed, n_sites, n_queries, repeat_frac=rep, n_seeds=40,
+                                          planted_into_sites=planted,
+                                          repeat_query_frac=0.2 if cfg == "slice-10-37" else 0.0)
+    idx_path = os.path.join(tmp, f"{name}.issl")
+    sorted_seqs = ref_build_index(sites, occ, SLICE_CONFIGS[cfg], idx_path, tmp)
+    # canonical site order: the reference builder's (sorted text) order
+    sig_sorted = np.array([synth.seq_to_sig(s) for s in sorted_seqs], np.uint64)
+    occ_map = dict(zip(sites.tolist(), occ.tolist()))
+    occ_sorted = np.array([occ_map[int(s)] for s in sig_sorted], np.uint32)
+    digest = hashlib.sha256(open(idx_path, "rb").read()).hexdigest()
+    qseqs = [synth.sig_to_seq(q) for q in queries.tolist()]
+    # 23-mer guides (protospacer + NGG) for the module path: only the first 20 nt are scored
+    guides = [q + "AGG" for q in qseqs]
+    arrays = {"sites": sig_sorted, "occ": occ_sorted, "queries": queries.astype(np.uint64),
+              "masks": synth.masks_from_strings(SLICE_CONFIGS[cfg])}
+    meta = {"name": name, "config": cfg, "index_sha256": digest, "thresholds": THRESHOLDS,
+            "methods": MODULE_METHODS}
+    for meth in MODULE_METHODS:
+        for t in THRESHOLDS:
+            m, c, codes = ref_module(idx_path, guides, meth, t, tmp)
+            cnt, distinct = ref_cli(idx_path, qseqs, CLI_NAME[meth], t, tmp)
+            key = f"{meth}_{t}"
+            arrays[f"mit_{key}"] = m
+            arrays[f"cfd_{key}"] = c
+            arrays[f"code_{key}"] = codes
+            arrays[f"count_{key}"] = cnt
+            arrays[f"distinct_{key}"] = np.array([distinct], np.uint64)
+    np.savez_compressed(os.path.join(HERE, f"case_{name}.npz"), meta=json.dumps(meta), **arrays)
+    print(f"{name}: {len(sig_sorted)} sites, {len(queries)} queries, index {digest[:12]}")
+
+
+def make_tiny(tmp):
+    """The reference's own tiny genome fixture through the reference's own builder."""
+    fa = os.path.join(REF, "tests", "data", "test_genome_offTargets.fa")
+    sc = os.path.join(tmp, "s45.txt")
+    with open(sc, "w") as f:
+        f.write("\n".join(SLICE_CONFIGS["slice-4-5"]) + "\n")
+    shutil.copy(fa, os.path.join(tmp, "ot.txt"))
+    out = os.path.join(HERE, "tiny_genome.issl")
+    run([os.path.join(REF_BIN, "ISSLCreateIndex"), os.path.join(tmp, "ot.txt"), sc, "20", out], cwd=tmp)
+    sites = sorted(set(l.strip() for l in open(fa) if l.strip()))
+    qs = [l.strip() for l in open(os.path.join(REF, "sample", "test_queries.txt")) if l.strip()]
+    # the reference sample queries (blank lines removed), every indexed site, and one- and
+    # two-substitution variants of the first sites
+    variants = []
+    for s in sites[:12]:
+        v1 = s[:5] + ("A" if s[5] != "A" else "C") + s[6:]
+        v2 = v1[:13] + ("G" if v1[13] != "G" else "T") + v1[14:]
+        variants += [v1, v2]
+    queries = qs + sites + variants
+    arrays = {"queries": np.array([synth.seq_to_sig(q) for q in queries], np.uint64)}
+    meta = {"name": "tiny", "config": "slice-4-5", "thresholds": THRESHOLDS, "methods": MODULE_METHODS,
+            "index_sha256": hashlib.sha256(open(out, "rb").read()).hexdigest()}
+    guides = [q + "TGG" for q in queries]
+    # processGuide filter coverage: alternate uniqueness / consensus / bowtie2 flags
+    flags = [(i % 2, i % 4, "0" if i % 5 == 0 else "1") for i in range(len(guides))]
+    for meth in MODULE_METHODS:
+        for t in THRESHOLDS:
+            m, c, codes = ref_module(out, guides, meth, t, tmp)
+            cnt, distinct = ref_cli(out, queries, CLI_NAME[meth], t, tmp)
+            key = f"{meth}_{t}"
+            arrays[f"mit_{key}"], arrays[f"cfd_{key}"], arrays[f"code_{key}"] = m, c, codes
+            arrays[f"count_{key}"] = cnt
+            arrays[f"distinct_{key}"] = np.array([distinct], np.uint64)
+    for level in ["ultralow", "low", "medium", "high"]:
+        m, c, codes = ref_module(out, guides, "mitAndCfd", 75.0, tmp, optimisation=level, consensus_n=2,
+                                 flags=flags)
+        arrays[f"filter_mit_{level}"], arrays[f"filter_cfd_{level}"], arrays[f"filter_code_{level}"] = m, c, codes
+    arrays["filter_flags"] = np.array([[u, cn, ord(b)] for u, cn, b in flags], np.int64)
+    m, c, codes = ref_module(out, guides, "mitAndCfd", 75.0, tmp, enabled=0)
+    arrays["disabled_mit"], arrays["disabled_cfd"], arrays["disabled_code"] = m, c, codes
+    np.savez_compressed(os.path.join(HERE, "case_tiny.npz"), meta=json.dumps(meta), **arrays)
+    print(f"tiny: {len(sites)} sites, {len(queries)} queries")
+
+
+def main():
+    mit, pos, pam = parse_penalties()
+    hdr, legacy = legacy_mit_pairs()
+    assert len(mit) == 6195 and len(legacy) == 6195
+    assert sorted(mit) == sorted(legacy), "legacy index MIT pairs differ from otScorePenalties"
+    payload = {
+        "source": "lib/otScorePenalties.cpp (reference), cross-checked against the (mask, score) pairs "
+                  "embedded in tests/data/test_genome_offTargets_indexed.issl",
+        "legacy_header": list(hdr),
+        "legacy_pairs_equal": True,
+        "mit": [[k, v.hex()] for k, v in sorted(mit)],
+        "cfd_pos": [v.hex() for v in pos],
+        "cfd_pam": [v.hex() for v in pam],
+    }
+    with open(os.path.join(HERE, "penalties.json"), "w") as f:
+        json.dump(payload, f, indent=0)
+    print("penalties.json:", len(mit), "MIT pairs")
+    with tempfile.TemporaryDirectory() as tmp:
+        make_tiny(tmp)
+        for c in CASES:
+            make_case(*c, tmp)
+
+
+if __name__ == "__main__":
+    main()
