@@ -1,0 +1,383 @@
+"""Benchmark of ISSL off-target scoring on B200 (one JSON line on rank 0).
+
+Workload (default): 300,000,000 distinct 20-nt sites (95% i.i.d. GC 41%, 5% copies of 10,000
+repeat seeds with Poisson(2) substitutions), occurrences min(1+Geometric(0.9),255), indexed with
+the 20 x 8-nt slice-8-20 layout; 100,000 guides (half sampled sites with 0-4 planted substitutions,
+half random); MIT+CFD with the 'and' rule, threshold 75, max 4 mismatches. Synthetic, seeded,
+generated on the device. One step = scoring the whole 100,000-guide set.
+
+  value  guides/s with guides and outputs resident in HBM (issl_score_device), device time from
+         CUDA events on the scoring stream, max over ranks
+  e2e    guides/s through issl_score with pinned host buffers: ASCII guides copied in and scores,
+         codes and counts copied out inside every step
+  roofline  the scan kernel (k_scan): bytes it must move per launch / its event-timed duration,
+         against the measured HBM copy bandwidth
+  cpu_baseline  the CPU restatement of the reference algorithm (oracle/, OpenMP on all host
+         cores) on a bounded guide sample of the same index
+
+--impl reference runs the reference's own ISSLScoreOfftargets (compiled from the reference sources
+into oracle/_ref) on the same index, written as a .issl file, on all host cores.
+
+Multi-GPU (torchrun): every rank holds a replica of the index and scores its own 100,000 guides
+(weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "guides/sec (MIT+CFD, <=4 mm, 300M-site index, 1 B200)"
+WORKLOAD = {
+    "workload": "issl-score plain: 300M-site slice-8-20 index, 100k guides, MIT+CFD 'and', threshold 75, "
+                "max 4 mismatches",
+    "n_sites": 300_000_000,
+    "slice_config": "slice-8-20",
+    "n_queries": 100_000,
+    "method": "and",
+    "threshold": 75.0,
+    "max_dist": 4,
+    "repeat_frac": 0.05,
+    "repeat_seeds": 10_000,
+    "repeat_lambda": 2.0,
+    "seed": 1235,
+    "l2": "inputs larger than L2 (the 24 GB residual array streamed per step)",
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--sites", type=int, default=None, help="override the site count (smaller runs)")
+    ap.add_argument("--queries", type=int, default=None)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the scan kernel from the committed ncu summary, if present."""
+    p = os.path.join(REPO, "profiles", "k_scan_300M_slice-8-20.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_launch_full:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def spec_for(args, world):
+    import cracklingplusplus_gpu_b200 as pkg
+    n_sites = args.sites or WORKLOAD["n_sites"]
+    nq = args.queries or WORKLOAD["n_queries"]
+    return pkg.SynthSpec(seed=WORKLOAD["seed"], n_sites=n_sites, slice_config=WORKLOAD["slice_config"],
+                         n_queries=nq * world, repeat_frac=WORKLOAD["repeat_frac"],
+                         n_repeat_seeds=WORKLOAD["repeat_seeds"], repeat_lambda=WORKLOAD["repeat_lambda"],
+                         copied_frac=0.5), n_sites, nq
+
+
+def cpu_baseline_port(ix, queries, method_id, threshold, target_s, gpu_res=None):
+    """The oracle (C restatement of the reference loop, OpenMP on every host core) on a guide
+    sample of the same index, exported to host memory in the reference layout."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle")], check=True)
+    pen = json.load(open(os.path.join(REPO, "tests", "golden", "penalties.json")))
+    pyoracle.set_cfd_tables([float.fromhex(x) for x in pen["cfd_pos"]], [float.fromhex(x) for x in pen["cfd_pam"]])
+    sigs, masks, sizes, lists = ix.export()
+    oix = pyoracle.Index.from_arrays(sigs, masks, sizes, lists)
+    cores = os.cpu_count() or 1
+    probe = queries[: max(64, cores * 8)]
+    t0 = time.perf_counter()
+    oix.score(probe, method_id, threshold, threads=cores)
+    dt = time.perf_counter() - t0
+    n = int(min(len(queries), max(len(probe), target_s / max(dt / len(probe), 1e-9))))
+    sample = queries[:n]
+    t0 = time.perf_counter()
+    tm, tc, cnt, _ = oix.score(sample, method_id, threshold, threads=cores)
+    dt = time.perf_counter() - t0
+    parity = None
+    if gpu_res is not None:
+        ms, cs, codes = pyoracle.finalise(method_id, threshold, tm, tc)
+        rel = lambda a, b: float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))) if len(a) else 0.0
+        parity = {"sample": n, "codes_equal": bytes(gpu_res.code[:n]) == codes,
+                  "counts_equal": bool(np.array_equal(gpu_res.count[:n], cnt)),
+                  "max_rel_err_mit": rel(gpu_res.mit[:n], ms), "max_rel_err_cfd": rel(gpu_res.cfd[:n], cs)}
+    del oix, sigs, masks, sizes, lists
+    return {"value": n / dt, "unit": "guides/s", "cores": cores, "kind": "port",
+            "sample": f"first {n} of the {len(queries)} benchmark guides on the full index ({dt:.1f} s)"}, parity
+
+
+def run_ours(args):
+    import torch
+    import cracklingplusplus_gpu_b200 as pkg
+    from cracklingplusplus_gpu_b200 import build
+    world, rank, local = dist_env()
+    build.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    spec, n_sites, nq = spec_for(args, world)
+    t0 = time.time()
+    ix, allq = pkg.Index.synth(spec, device=local)
+    gen_s = time.time() - t0
+    q = np.ascontiguousarray(allq[rank * nq:(rank + 1) * nq])
+    method_id = pkg.CLI_METHODS[WORKLOAD["method"]]
+    thr, md = WORKLOAD["threshold"], WORKLOAD["max_dist"]
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    d_q = torch.from_numpy(q.view(np.int64)).to(dev)
+    d_mit = torch.empty(nq, dtype=torch.float64, device=dev)
+    d_cfd = torch.empty(nq, dtype=torch.float64, device=dev)
+    d_code = torch.empty(nq, dtype=torch.uint8, device=dev)
+    d_cnt = torch.empty(nq, dtype=torch.int64, device=dev)
+    d_dist = torch.empty(1, dtype=torch.int64, device=dev)
+
+    def step_device():
+        ix.score_device(d_q.data_ptr(), nq, method_id, thr, md, d_mit.data_ptr(), d_cfd.data_ptr(),
+                        d_code.data_ptr(), d_cnt.data_ptr(), d_dist.data_ptr(), stream.cuda_stream)
+
+    # ---- device-resident throughput -------------------------------------------------------
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    scan_ms, scan_bytes, launches = [], [], 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step_device()
+            st = ix.last_stats()
+            scan_ms.append(st.scan_ms)
+            scan_bytes.append(st.scan_bytes)
+            launches += st.launches
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * nq * args.steps / (ms / 1e3)
+
+    # ---- end to end through the public API with pinned host buffers -------------------------
+    from cracklingplusplus_gpu_b200.index import decode
+    ascii_np = np.frombuffer(b"".join(decode(s).encode() + b"\n" for s in q), dtype=np.uint8)
+    h_in = torch.from_numpy(ascii_np.copy()).pin_memory()
+    h_mit = torch.empty(nq, dtype=torch.float64).pin_memory()
+    h_cfd = torch.empty(nq, dtype=torch.float64).pin_memory()
+    h_code = torch.empty(nq, dtype=torch.uint8).pin_memory()
+    h_cnt = torch.empty(nq, dtype=torch.int64).pin_memory()
+    import ctypes as C
+    L = pkg.lib()
+    u64p, f64p = C.POINTER(C.c_uint64), C.POINTER(C.c_double)
+    dist_out = (C.c_uint64 * 1)()
+
+    def step_e2e():
+        rc = L.issl_score(ix.handle, C.c_char_p(h_in.data_ptr()), 21, nq, method_id, thr, md,
+                          C.cast(h_mit.data_ptr(), f64p), C.cast(h_cfd.data_ptr(), f64p),
+                          C.c_char_p(h_code.data_ptr()), C.cast(h_cnt.data_ptr(), u64p), dist_out)
+        if rc != 0:
+            raise RuntimeError(L.issl_last_error())
+
+    for _ in range(args.warmup):
+        step_e2e()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_e2e()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * nq * args.steps / e2e_s
+
+    # results of the last e2e step, for the CPU parity sample
+    gpu_res = pkg.ScoreResult(h_mit.numpy().copy(), h_cfd.numpy().copy(), bytes(h_code.numpy()), h_cnt.numpy().view(
+        np.uint64).copy(), int(dist_out[0]))
+
+    peak, peak_kind = measured_peaks()
+    scan_avg_ms = sum(scan_ms) / len(scan_ms)
+    bytes_per_launch = sum(scan_bytes) / len(scan_bytes)
+    achieved = bytes_per_launch / (scan_avg_ms / 1e3) / 1e9
+    traffic = committed_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "guides/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32/u64 integer scan, f64 sums", "data": "synthetic (seeded, generated on device)",
+        "config": dict(WORKLOAD, n_sites=n_sites, n_queries=nq, parallelism=f"replicas{world}" if world > 1 else "1 GPU"),
+        "e2e": {"value": e2e_value, "unit": "guides/s", "h2d_bytes_per_step": int(len(ascii_np)),
+                "d2h_bytes_per_step": int(nq * (8 + 8 + 1 + 8) + 8)},
+        "roofline": {"bound": "hbm", "kernel": "k_scan", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "bytes_per_launch": bytes_per_launch, "kernel_ms": scan_avg_ms},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "probes_per_s": value * len(__import__("cracklingplusplus_gpu_b200").slice_masks(WORKLOAD["slice_config"])),
+        "generation_s": gen_s,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu, parity = cpu_baseline_port(ix, q, method_id, thr, args.cpu_seconds, gpu_res)
+        line["cpu_baseline"] = cpu
+        line["parity_sample"] = parity
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    ix.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args):
+    """The reference's own CPU scorer on the same workload, all host cores."""
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    binary = os.path.join(REPO, "oracle", "_ref", "ISSLScoreOfftargets")
+    spec_sites = args.sites or WORKLOAD["n_sites"]
+    if not os.path.exists(binary):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ISSLScoreOfftargets was not built "
+                          "(needs the reference sources at build time)"}))
+        return
+    import cracklingplusplus_gpu_b200 as pkg
+    from cracklingplusplus_gpu_b200 import build
+    from cracklingplusplus_gpu_b200.index import decode
+    build.build()
+    spec, n_sites, nq = spec_for(args, 1)
+    ix, q = pkg.Index.synth(spec, device=local)
+    cores = os.cpu_count() or 1
+    workdir = tempfile.mkdtemp(dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        idx = os.path.join(workdir, "index.issl")
+        ix.save(idx)
+        ix.close()
+        # bounded sample: K steps of `per_step` guides scored in one invocation of the reference
+        per_step = max(64, int(os.environ.get("ISSL_REF_GUIDES_PER_STEP", "0")) or (200 if spec_sites >= 10**8 else 1000))
+        total = per_step * args.steps
+        sample = q[:total]
+        qf = os.path.join(workdir, "queries.txt")
+        with open(qf, "w") as f:
+            f.write("".join(decode(s) + "\n" for s in sample))
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+        r = subprocess.run([binary, idx, qf, "4", str(WORKLOAD["threshold"]), WORKLOAD["method"], "out.txt"],
+                           cwd=workdir, env=env, capture_output=True, text=True)
+        if r.returncode != 0:
+            print(json.dumps({"impl": "reference", "unavailable": f"reference exited {r.returncode}: "
+                              f"{r.stderr.strip()[-200:]}"}))
+            return
+        t = float(re.search(r"ISSL scoring time: ([0-9.eE+-]+) seconds", r.stdout).group(1))
+    finally:
+        shutil.rmtree(workdir, ignore_errors=True)
+    value = len(sample) / t
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "guides/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 integer scan, f64 sums", "data": "synthetic",
+        "config": dict(WORKLOAD, n_sites=n_sites, n_queries=nq, parallelism="host cores"),
+        "cpu_baseline": {"value": value, "unit": "guides/s", "cores": cores, "kind": "reference",
+                         "sample": f"{len(sample)} guides ({per_step} per step) of the benchmark set on the full "
+                                   f"index; the reference's own 'ISSL scoring time'"},
+        "e2e": {"value": value, "unit": "guides/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

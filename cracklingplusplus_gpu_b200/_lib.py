@@ -1,0 +1,103 @@
+"""ctypes bindings of libissl_b200.so (the C ABI of include/issl_b200.h and issl_b200_module.hpp)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_NAME = "libissl_b200.so"
+
+# otScoreMethod, include/util.hpp:20 (and the INI names of lib/util.cpp:13-19)
+OT_METHODS = {"mit": 0, "cfd": 1, "mitAndCfd": 2, "mitOrCfd": 3, "avgMitCfd": 4}
+# method words of the ISSLScoreOfftargets command line (ISSLScoreOfftargets.cpp:69-91)
+CLI_METHODS = {"mit": 0, "cfd": 1, "and": 2, "or": 3, "avg": 4}
+
+STATUS = {0: "ok", -1: "invalid argument", -2: "I/O error", -3: "format error", -4: "out of memory",
+          -5: "CUDA error", -6: "timeout", -7: "unsupported", -8: "busy"}
+
+
+class IsslError(RuntimeError):
+    """A failing library call: .code is the ISSL_ERR_* status, str() the library's message."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} [{STATUS.get(code, code)}]")
+        self.code = code
+
+
+class IndexInfo(C.Structure):
+    _fields_ = [("n_sites", C.c_uint64), ("seq_len", C.c_uint64), ("n_slices", C.c_uint64),
+                ("n_buckets", C.c_uint64), ("device_bytes", C.c_uint64), ("device", C.c_int),
+                ("min_width", C.c_int), ("max_width", C.c_int)]
+
+
+class ScoreStats(C.Structure):
+    _fields_ = [("scan_ms", C.c_double), ("total_ms", C.c_double), ("probes", C.c_uint64),
+                ("buckets_scanned", C.c_uint64), ("entries_scanned", C.c_uint64), ("units", C.c_uint64),
+                ("hits", C.c_uint64), ("scan_bytes", C.c_uint64), ("launches", C.c_uint64)]
+
+
+class SynthSpecC(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("n_sites", C.c_uint64), ("repeat_frac", C.c_double),
+                ("n_repeat_seeds", C.c_uint64), ("repeat_lambda", C.c_double), ("n_queries", C.c_uint64),
+                ("copied_frac", C.c_double), ("repeat_query_frac", C.c_double), ("planted_into_sites", C.c_int),
+                ("slice_masks", C.POINTER(C.c_uint64)), ("n_slices", C.c_uint64)]
+
+
+def library_path() -> str:
+    return os.path.join(HERE, _LIB_NAME)
+
+
+_lib = None
+
+P = C.POINTER
+u64p = P(C.c_uint64)
+f64p = P(C.c_double)
+vp = C.c_void_p
+
+# (name, restype, argtypes) of every exported entry point
+SIGNATURES = [
+    ("issl_last_error", C.c_char_p, []),
+    ("issl_open", C.c_int, [C.c_char_p, C.c_int, P(vp)]),
+    ("issl_open_arrays", C.c_int, [u64p, C.c_uint64, C.c_uint64, u64p, C.c_uint64, u64p, u64p, C.c_int, P(vp)]),
+    ("issl_build", C.c_int, [u64p, P(C.c_uint32), C.c_uint64, u64p, C.c_uint64, C.c_int, P(vp)]),
+    ("issl_close", C.c_int, [vp]),
+    ("issl_index_get_info", C.c_int, [vp, P(IndexInfo)]),
+    ("issl_export", C.c_int, [vp, u64p, u64p, u64p, u64p]),
+    ("issl_save", C.c_int, [vp, C.c_char_p]),
+    ("issl_score", C.c_int, [vp, C.c_char_p, C.c_size_t, C.c_size_t, C.c_int, C.c_double, C.c_int, f64p, f64p,
+                             C.c_char_p, u64p, u64p]),
+    ("issl_score_sigs", C.c_int, [vp, u64p, C.c_size_t, C.c_int, C.c_double, C.c_int, f64p, f64p, C.c_char_p,
+                                  u64p, u64p]),
+    ("issl_score_device", C.c_int, [vp, vp, C.c_size_t, C.c_int, C.c_double, C.c_int, vp, vp, vp, vp, vp, vp]),
+    ("issl_last_stats", C.c_int, [vp, P(ScoreStats)]),
+    ("issl_synth", C.c_int, [P(SynthSpecC), C.c_int, P(vp), u64p]),
+    ("issl_tables", C.c_int, [u64p, f64p, f64p, f64p]),
+    ("issl_module_run", C.c_int, [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_size_t,
+                                  C.c_char_p, C.c_size_t, P(C.c_uint8), P(C.c_int8), C.c_char_p, f64p, f64p,
+                                  C.c_char_p]),
+    ("issl_module_release_all", C.c_int, []),
+]
+
+
+def lib():
+    """The loaded native library; raises ImportError when it has not been built."""
+    global _lib
+    if _lib is None:
+        path = library_path()
+        if not os.path.exists(path):
+            raise ImportError(
+                f"{path} is missing: build the CUDA library first "
+                "(python -m cracklingplusplus_gpu_b200.build); there is no CPU fallback")
+        L = C.CDLL(path)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        msg = lib().issl_last_error()
+        raise IsslError(rc, msg.decode(errors="replace") if msg else "error")

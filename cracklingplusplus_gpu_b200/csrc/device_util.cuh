@@ -1,0 +1,43 @@
+// Bit manipulation shared by the index builder and the scoring kernels.
+#pragma once
+#include <cstdint>
+
+#include "issl_internal.cuh"
+
+namespace issl {
+
+// Slice key of a signature: the 2-bit bases at the slice positions, packed in ascending
+// position order (ISSLScoringModule.cpp:235-239, ISSLCreateIndex.cpp:458-462).
+__host__ __device__ __forceinline__ uint32_t slice_key(uint64_t sig, const SliceGeom& g) {
+    uint32_t key = 0;
+    for (int j = 0; j < g.width; j++) key |= static_cast<uint32_t>((sig >> (2 * g.pos[j])) & 3u) << (2 * j);
+    return key;
+}
+
+// Residual code: the bases outside the slice packed the same way (at most 32 bits for
+// slices of width >= 4).
+__host__ __device__ __forceinline__ uint32_t slice_residual(uint64_t sig, const SliceGeom& g) {
+    uint32_t r = 0;
+    for (int j = 0; j < g.rwidth; j++) r |= static_cast<uint32_t>((sig >> (2 * g.rpos[j])) & 3u) << (2 * j);
+    return r;
+}
+
+// One bit per mismatching base pair, at the even bit of each 2-bit field. Equivalent to
+// ((x & 0xAA..) >> 1) | (x & 0x55..) of ISSLScoringModule.cpp:287-289.
+__host__ __device__ __forceinline__ uint64_t fold64(uint64_t x) {
+    return (x | (x >> 1)) & 0x5555555555555555ull;
+}
+__host__ __device__ __forceinline__ uint32_t fold32(uint32_t x) { return (x | (x >> 1)) & 0x55555555u; }
+
+// 40-bit even-bit mismatch mask -> 20-bit position mask.
+__host__ __device__ __forceinline__ uint32_t compress_even40(uint64_t m) {
+    m &= 0x5555555555555555ull;
+    m = (m | (m >> 1)) & 0x3333333333333333ull;
+    m = (m | (m >> 2)) & 0x0F0F0F0F0F0F0F0Full;
+    m = (m | (m >> 4)) & 0x00FF00FF00FF00FFull;
+    m = (m | (m >> 8)) & 0x0000FFFF0000FFFFull;
+    m = (m | (m >> 16)) & 0x00000000FFFFFFFFull;
+    return static_cast<uint32_t>(m);
+}
+
+}  // namespace issl

@@ -1,0 +1,569 @@
+// The resident index: .issl loading, validation, GPU construction and export.
+//
+// Device layout (slice-major, list order of the reference file kept):
+//   sigs    [N]      u64  2-bit packed site signatures (the file's offtargets array)
+//   occ     [N]      u32  occurrence count per site (the high word of every list entry)
+//   ids     [S*N]    u32  site id per list entry (the low word of every list entry)
+//   resid   [S*N+4]  u32  residual code per list entry: the site's bases outside the slice
+//   offsets [G+1]    u64  bucket starts in global entry numbering (slice s, position j -> s*N + j);
+//                         buckets are numbered slice by slice, so off[g+1] - off[g] is always the
+//                         size of bucket g, across slice boundaries too
+// The reference stores (occ << 32) | id per entry and gathers offtargets[id] for every entry it
+// scans (ISSLScoringModule.cpp:248-286). Here the scan streams resid only (4 bytes per entry)
+// because the slice positions of every entry in a bucket equal the query's by construction.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "device_util.cuh"
+#include "issl_internal.cuh"
+#include "scan.cuh"
+
+namespace issl {
+
+namespace {
+thread_local std::string g_last_error;
+}
+void set_last_error(const std::string& m) { g_last_error = m; }
+
+std::vector<SliceGeom> make_geometry(const std::vector<uint64_t>& masks, uint64_t seq_len) {
+    ISSL_REQUIRE(seq_len >= 1 && seq_len <= kSeqLen, ISSL_ERR_UNSUPPORTED,
+                 "only indexes of 20-nt (or shorter) sites are supported, got seqLength " +
+                     std::to_string(seq_len));
+    ISSL_REQUIRE(!masks.empty() && masks.size() <= static_cast<size_t>(kMaxSlices), ISSL_ERR_UNSUPPORTED,
+                 "slice count must be 1.." + std::to_string(kMaxSlices) + ", got " +
+                     std::to_string(masks.size()));
+    std::vector<SliceGeom> geom(masks.size());
+    uint64_t bbase = 0;
+    const uint64_t valid = (1ull << seq_len) - 1;
+    for (size_t s = 0; s < masks.size(); s++) {
+        SliceGeom& g = geom[s];
+        std::memset(&g, 0, sizeof g);
+        const uint64_t pm = masks[s] & valid;  // positions >= seqLength are ignored (:107-113)
+        g.pmask = static_cast<uint32_t>(pm);
+        int w = 0, r = 0;
+        for (int p = 0; p < kSeqLen; p++) {
+            if (pm >> p & 1u)
+                g.pos[w++] = static_cast<uint8_t>(p);
+            else
+                g.rpos[r++] = static_cast<uint8_t>(p);
+        }
+        ISSL_REQUIRE(w >= 4 && w <= 13, ISSL_ERR_UNSUPPORTED,
+                     "slice " + std::to_string(s) + " has width " + std::to_string(w) +
+                         "; supported widths are 4..13 positions");
+        g.width = static_cast<uint8_t>(w);
+        g.rwidth = static_cast<uint8_t>(r);
+        g.bbase = static_cast<uint32_t>(bbase);
+        bbase += 1ull << (2 * w);
+        ISSL_REQUIRE(bbase + masks.size() + 1 < (1ull << 32), ISSL_ERR_UNSUPPORTED,
+                     "too many buckets over all slices");
+    }
+    return geom;
+}
+
+namespace {
+
+__global__ void k_slice_keys(const uint64_t* __restrict__ sigs, uint64_t n, SliceGeom g,
+                             uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        keys[i] = slice_key(sigs[i], g);
+        vals[i] = static_cast<uint32_t>(i);
+    }
+}
+
+// off[k] = base + first position whose key >= k, for k in [0, nb]; keys sorted ascending.
+__global__ void k_offsets_from_sorted(const uint32_t* __restrict__ keys, uint64_t n, uint32_t nb, uint64_t base,
+                                      uint64_t* __restrict__ off) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i <= n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const int64_t prev = i == 0 ? -1 : static_cast<int64_t>(keys[i - 1]);
+        const int64_t cur = i == n ? static_cast<int64_t>(nb) : static_cast<int64_t>(keys[i]);
+        for (int64_t k = prev + 1; k <= cur; k++) off[k] = base + i;
+    }
+}
+
+__global__ void k_resid(const uint32_t* __restrict__ ids, const uint64_t* __restrict__ sigs, uint64_t n,
+                        SliceGeom g, uint32_t* __restrict__ resid) {
+    for (uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; j < n;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        resid[j] = slice_residual(sigs[ids[j]], g);
+}
+
+// bucket_of[j] for every list position j of one slice (off: the slice's nb+1 global starts)
+__global__ void k_fill_bucket_of(const uint64_t* __restrict__ off, uint32_t nb, uint64_t base,
+                                 uint32_t* __restrict__ bucket_of) {
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < nb;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        for (uint64_t j = off[k] - base; j < off[k + 1] - base; j++) bucket_of[j] = static_cast<uint32_t>(k);
+}
+
+enum : uint32_t { kBadId = 1u, kDupId = 2u, kOccMismatch = 4u, kWrongBucket = 8u };
+
+// Splits file entries (occ << 32 | id) of slice s, list positions [j0, j0+cnt), into ids/occ and
+// validates them: id < N, each id once per slice, one occurrence count per site across slices,
+// and the entry sits in the bucket of its own slice key.
+__global__ void k_split_entries(const uint64_t* __restrict__ entries, uint64_t j0, uint64_t cnt, uint64_t n_sites,
+                                int first_slice, SliceGeom g, const uint64_t* __restrict__ sigs,
+                                const uint32_t* __restrict__ bucket_of, uint32_t* __restrict__ ids_slice,
+                                uint32_t* __restrict__ occ, uint32_t* __restrict__ seen, uint32_t* flags) {
+    for (uint64_t t = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; t < cnt;
+         t += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t e = entries[t];
+        const uint64_t id = e & 0xFFFFFFFFull;
+        const uint32_t o = static_cast<uint32_t>(e >> 32);
+        const uint64_t j = j0 + t;
+        if (id >= n_sites) {
+            atomicOr(flags, kBadId);
+            ids_slice[j] = 0;
+            continue;
+        }
+        ids_slice[j] = static_cast<uint32_t>(id);
+        const uint32_t bit = 1u << (id & 31);
+        if (atomicOr(&seen[id >> 5], bit) & bit) atomicOr(flags, kDupId);
+        if (first_slice)
+            occ[id] = o;
+        else if (occ[id] != o)
+            atomicOr(flags, kOccMismatch);
+        if (slice_key(sigs[id], g) != bucket_of[j]) atomicOr(flags, kWrongBucket);
+    }
+}
+
+__global__ void k_join_entries(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ occ, uint64_t cnt,
+                               uint64_t* __restrict__ out) {
+    for (uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; j < cnt;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t id = ids[j];
+        out[j] = (static_cast<uint64_t>(occ[id]) << 32) | id;
+    }
+}
+
+inline unsigned grid_for(uint64_t n, unsigned threads = 256) {
+    uint64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148ull * 32) b = 148ull * 32;
+    return static_cast<unsigned>(b);
+}
+
+uint64_t count_buckets(const std::vector<SliceGeom>& g) {
+    uint64_t t = 0;
+    for (auto& s : g) t += 1ull << (2 * s.width);
+    return t;
+}
+
+// ---- sequential sources for the loader: the .issl byte stream, from a file or from arrays ----
+struct Source {
+    virtual ~Source() = default;
+    virtual void read(void* dst, size_t bytes, const char* what) = 0;
+};
+
+struct FileSource : Source {
+    FILE* fp;
+    explicit FileSource(const char* path) : fp(std::fopen(path, "rb")) {
+        ISSL_REQUIRE(fp != nullptr, ISSL_ERR_IO, std::string("Error reading index: could not open file ") + path);
+    }
+    ~FileSource() override {
+        if (fp) std::fclose(fp);
+    }
+    void read(void* dst, size_t bytes, const char* what) override {
+        if (bytes == 0) return;
+        ISSL_REQUIRE(std::fread(dst, 1, bytes, fp) == bytes, ISSL_ERR_IO,
+                     std::string("Error reading index: ") + what + " (file truncated)");
+    }
+};
+
+struct ArraySource : Source {
+    // segments of the virtual stream in order
+    std::vector<std::pair<const uint8_t*, size_t>> segs;
+    size_t seg = 0, off = 0;
+    void read(void* dst, size_t bytes, const char* what) override {
+        uint8_t* d = static_cast<uint8_t*>(dst);
+        while (bytes) {
+            ISSL_REQUIRE(seg < segs.size(), ISSL_ERR_ARG, std::string("index arrays too short: ") + what);
+            const size_t take = std::min(bytes, segs[seg].second - off);
+            std::memcpy(d, segs[seg].first + off, take);
+            d += take;
+            bytes -= take;
+            off += take;
+            if (off == segs[seg].second) {
+                seg++;
+                off = 0;
+            }
+        }
+    }
+};
+
+struct PinnedStaging {
+    static constexpr size_t kBytes = 64ull << 20;
+    void* h[2] = {nullptr, nullptr};
+    uint64_t* d[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    PinnedStaging() {
+        for (int i = 0; i < 2; i++) {
+            ISSL_CUDA(cudaMallocHost(&h[i], kBytes));
+            ISSL_CUDA(cudaMalloc(reinterpret_cast<void**>(&d[i]), kBytes));
+            ISSL_CUDA(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming));
+        }
+    }
+    ~PinnedStaging() {
+        for (int i = 0; i < 2; i++) {
+            if (h[i]) cudaFreeHost(h[i]);
+            if (d[i]) cudaFree(d[i]);
+            if (done[i]) cudaEventDestroy(done[i]);
+        }
+    }
+};
+
+void load_stream(issl_index* ix, Source& src, int device) {
+    ISSL_CUDA(cudaSetDevice(device));
+    ix->device = device;
+    uint64_t hdr[3];
+    src.read(hdr, sizeof hdr, "header invalid");
+    ix->n_sites = hdr[0];
+    ix->seq_len = hdr[1];
+    ix->n_slices = hdr[2];
+    ISSL_REQUIRE(ix->n_sites < (1ull << 32), ISSL_ERR_FORMAT, "index has 2^32 or more sites");
+    ISSL_REQUIRE(ix->n_slices >= 1 && ix->n_slices <= static_cast<uint64_t>(kMaxSlices), ISSL_ERR_FORMAT,
+                 "Error reading index: header invalid (slice count " + std::to_string(ix->n_slices) + ")");
+    ISSL_REQUIRE(ix->seq_len >= 1 && ix->seq_len <= 64, ISSL_ERR_FORMAT, "Error reading index: header invalid");
+    const uint64_t N = ix->n_sites, S = ix->n_slices;
+    cudaStream_t st;
+    ISSL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{st};
+    PinnedStaging stg;
+    const size_t per = PinnedStaging::kBytes / 8;
+
+    // signatures
+    ix->sigs.reserve(N);
+    for (uint64_t i = 0, b = 0; i < N; b ^= 1) {
+        const uint64_t cnt = std::min<uint64_t>(per, N - i);
+        ISSL_CUDA(cudaEventSynchronize(stg.done[b]));
+        src.read(stg.h[b], cnt * 8, "loading off-target sequences failed");
+        ISSL_CUDA(cudaMemcpyAsync(ix->sigs.p + i, stg.h[b], cnt * 8, cudaMemcpyHostToDevice, st));
+        ISSL_CUDA(cudaEventRecord(stg.done[b], st));
+        i += cnt;
+    }
+    ix->masks.resize(S);
+    src.read(ix->masks.data(), S * 8, "reading slice masks failed");
+    ix->geom = make_geometry(ix->masks, ix->seq_len);
+    ix->n_buckets = count_buckets(ix->geom);
+    ix->d_geom.reserve(S);
+    ISSL_CUDA(cudaMemcpyAsync(ix->d_geom.p, ix->geom.data(), S * sizeof(SliceGeom), cudaMemcpyHostToDevice, st));
+
+    ix->occ.reserve(N);
+    ix->ids.reserve(S * N);
+    ix->resid.reserve(S * N + 4);
+    ix->offsets.reserve(ix->n_buckets + 1);
+    ISSL_CUDA(cudaMemsetAsync(ix->resid.p + S * N, 0, 16, st));
+    DevBuf<uint32_t> seen, bucket_of, flags;
+    seen.reserve(N / 32 + 1);
+    bucket_of.reserve(N);
+    flags.reserve(1);
+    ISSL_CUDA(cudaMemsetAsync(flags.p, 0, 4, st));
+    std::vector<uint64_t> sizes, off64;
+    uint64_t bbase = 0;
+    for (uint64_t s = 0; s < S; s++) {
+        const SliceGeom& g = ix->geom[s];
+        const uint64_t nb = 1ull << (2 * g.width);
+        sizes.resize(nb);
+        src.read(sizes.data(), nb * 8, "reading slice list sizes failed");
+        off64.resize(nb + 1);
+        uint64_t acc = 0;
+        for (uint64_t k = 0; k < nb; k++) {
+            off64[k] = s * N + acc;
+            acc += sizes[k];
+            ISSL_REQUIRE(acc <= N, ISSL_ERR_FORMAT,
+                         "Error reading index: slice " + std::to_string(s) + " list sizes exceed the site count");
+        }
+        ISSL_REQUIRE(acc == N, ISSL_ERR_FORMAT,
+                     "Error reading index: slice " + std::to_string(s) + " list sizes sum to " +
+                         std::to_string(acc) + ", expected " + std::to_string(N));
+        off64[nb] = s * N + N;  // = first start of the next slice
+        // the previous slice's kernels read bucket_of / seen: order through the stream
+        ISSL_CUDA(cudaMemcpyAsync(ix->offsets.p + bbase, off64.data(), (nb + 1) * 8, cudaMemcpyHostToDevice, st));
+        ISSL_CUDA(cudaStreamSynchronize(st));  // off64 is reused next slice
+        k_fill_bucket_of<<<grid_for(nb), 256, 0, st>>>(ix->offsets.p + bbase, static_cast<uint32_t>(nb), s * N,
+                                                      bucket_of.p);
+        ISSL_CUDA(cudaMemsetAsync(seen.p, 0, (N / 32 + 1) * 4, st));
+        for (uint64_t j = 0, b = 0; j < N; b ^= 1) {
+            const uint64_t cnt = std::min<uint64_t>(per, N - j);
+            ISSL_CUDA(cudaEventSynchronize(stg.done[b]));
+            src.read(stg.h[b], cnt * 8, "reading slice contents failed");
+            ISSL_CUDA(cudaMemcpyAsync(stg.d[b], stg.h[b], cnt * 8, cudaMemcpyHostToDevice, st));
+            k_split_entries<<<grid_for(cnt), 256, 0, st>>>(stg.d[b], j, cnt, N, s == 0, g, ix->sigs.p, bucket_of.p,
+                                                           ix->ids.p + s * N, ix->occ.p, seen.p, flags.p);
+            ISSL_CUDA(cudaEventRecord(stg.done[b], st));
+            j += cnt;
+        }
+        k_resid<<<grid_for(N), 256, 0, st>>>(ix->ids.p + s * N, ix->sigs.p, N, g, ix->resid.p + s * N);
+        ISSL_CUDA(cudaGetLastError());
+        uint32_t f = 0;
+        ISSL_CUDA(cudaMemcpyAsync(&f, flags.p, 4, cudaMemcpyDeviceToHost, st));
+        ISSL_CUDA(cudaStreamSynchronize(st));
+        const std::string where = "Error reading index: slice " + std::to_string(s) + ": ";
+        ISSL_REQUIRE(!(f & kBadId), ISSL_ERR_FORMAT, where + "site id out of range");
+        ISSL_REQUIRE(!(f & kDupId), ISSL_ERR_FORMAT, where + "a site id is listed twice");
+        ISSL_REQUIRE(!(f & kOccMismatch), ISSL_ERR_FORMAT,
+                     where + "occurrence count of a site differs from slice 0 (unsupported)");
+        ISSL_REQUIRE(!(f & kWrongBucket), ISSL_ERR_FORMAT, where + "a site is listed under a bucket other than its key");
+        bbase += nb;
+    }
+    ISSL_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace
+
+void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint32_t* d_occ, cudaStream_t st) {
+    const uint64_t N = ix->n_sites, S = ix->n_slices;
+    ISSL_REQUIRE(N < (1ull << 32), ISSL_ERR_UNSUPPORTED, "2^32 or more sites");
+    ix->geom = make_geometry(ix->masks, ix->seq_len);
+    ix->n_buckets = count_buckets(ix->geom);
+    if (ix->sigs.p != d_sigs) {
+        ix->sigs.reserve(N);
+        ISSL_CUDA(cudaMemcpyAsync(ix->sigs.p, d_sigs, N * 8, cudaMemcpyDeviceToDevice, st));
+    }
+    if (ix->occ.p != d_occ) {
+        ix->occ.reserve(N);
+        ISSL_CUDA(cudaMemcpyAsync(ix->occ.p, d_occ, N * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    ix->d_geom.reserve(S);
+    ISSL_CUDA(cudaMemcpyAsync(ix->d_geom.p, ix->geom.data(), S * sizeof(SliceGeom), cudaMemcpyHostToDevice, st));
+    ix->ids.reserve(S * N);
+    ix->resid.reserve(S * N + 4);
+    ix->offsets.reserve(ix->n_buckets + 1);
+    ISSL_CUDA(cudaMemsetAsync(ix->resid.p + S * N, 0, 16, st));
+    DevBuf<uint32_t> keys, vals, keys2, vals2;
+    DevBuf<uint8_t> temp;
+    keys.reserve(N);
+    vals.reserve(N);
+    keys2.reserve(N);
+    vals2.reserve(N);
+    const size_t tb = radix_sort_temp_bytes(N, false);
+    temp.reserve(tb);
+    uint64_t bbase = 0;
+    for (uint64_t s = 0; s < S; s++) {
+        const SliceGeom& g = ix->geom[s];
+        const uint32_t nb = 1u << (2 * g.width);
+        k_slice_keys<<<grid_for(N), 256, 0, st>>>(ix->sigs.p, N, g, keys.p, vals.p);
+        uint32_t *ko = keys.p, *vo = vals.p;
+        // stable by key: ids stay ascending inside each bucket (ISSLCreateIndex.cpp:455-468)
+        radix_sort_pairs_u32(keys.p, vals.p, keys2.p, vals2.p, N, 2 * g.width, temp.p, tb, st, &ko, &vo);
+        if (N) ISSL_CUDA(cudaMemcpyAsync(ix->ids.p + s * N, vo, N * 4, cudaMemcpyDeviceToDevice, st));
+        k_offsets_from_sorted<<<grid_for(N + 1), 256, 0, st>>>(ko, N, nb, s * N, ix->offsets.p + bbase);
+        k_resid<<<grid_for(N), 256, 0, st>>>(ix->ids.p + s * N, ix->sigs.p, N, g, ix->resid.p + s * N);
+        ISSL_CUDA(cudaGetLastError());
+        bbase += nb;
+    }
+    ISSL_CUDA(cudaStreamSynchronize(st));
+}
+
+void export_slice_lists(const issl_index* ix, uint64_t s, uint64_t* host_lists, cudaStream_t st) {
+    const uint64_t N = ix->n_sites;
+    if (!N) return;
+    DevBuf<uint64_t> tmp;
+    tmp.reserve(N);
+    k_join_entries<<<grid_for(N), 256, 0, st>>>(ix->ids.p + s * N, ix->occ.p, N, tmp.p);
+    ISSL_CUDA(cudaGetLastError());
+    ISSL_CUDA(cudaMemcpyAsync(host_lists, tmp.p, N * 8, cudaMemcpyDeviceToHost, st));
+    ISSL_CUDA(cudaStreamSynchronize(st));
+}
+
+std::vector<uint64_t> export_sizes(const issl_index* ix) {
+    std::vector<uint64_t> sizes;
+    sizes.reserve(ix->n_buckets);
+    std::vector<uint64_t> off(ix->n_buckets + 1);
+    ISSL_CUDA(cudaMemcpy(off.data(), ix->offsets.p, (ix->n_buckets + 1) * 8, cudaMemcpyDeviceToHost));
+    for (uint64_t g = 0; g < ix->n_buckets; g++) sizes.push_back(off[g + 1] - off[g]);
+    return sizes;
+}
+
+}  // namespace issl
+
+issl::IndexView issl_index::view() const {
+    issl::IndexView v;
+    v.sigs = sigs.p;
+    v.occ = occ.p;
+    v.ids = ids.p;
+    v.resid = resid.p;
+    v.offsets = offsets.p;
+    v.geom = d_geom.p;
+    v.n_sites = n_sites;
+    v.n_slices = static_cast<uint32_t>(n_slices);
+    v.n_buckets = static_cast<uint32_t>(n_buckets);
+    return v;
+}
+
+using issl::guarded;
+
+extern "C" {
+
+const char* issl_last_error(void) { return issl::g_last_error.c_str(); }
+
+int issl_open(const char* path, int device, issl_index** out) {
+    return guarded([&] {
+        ISSL_REQUIRE(path && out, ISSL_ERR_ARG, "issl_open: null argument");
+        *out = nullptr;
+        auto ix = std::make_unique<issl_index>();
+        issl::FileSource src(path);
+        issl::load_stream(ix.get(), src, device);
+        *out = ix.release();
+    });
+}
+
+int issl_open_arrays(const uint64_t* sigs, uint64_t n_sites, uint64_t seq_len, const uint64_t* slice_masks,
+                     uint64_t n_slices, const uint64_t* list_sizes, const uint64_t* lists, int device,
+                     issl_index** out) {
+    return guarded([&] {
+        ISSL_REQUIRE(out && slice_masks && list_sizes && (lists || n_sites == 0) && (sigs || n_sites == 0),
+                     ISSL_ERR_ARG, "issl_open_arrays: null argument");
+        *out = nullptr;
+        ISSL_REQUIRE(n_slices >= 1 && n_slices <= static_cast<uint64_t>(issl::kMaxSlices), ISSL_ERR_ARG,
+                     "issl_open_arrays: slice count out of range");
+        static thread_local uint64_t hdr[3];
+        hdr[0] = n_sites;
+        hdr[1] = seq_len;
+        hdr[2] = n_slices;
+        issl::ArraySource src;
+        src.segs.push_back({reinterpret_cast<const uint8_t*>(hdr), sizeof hdr});
+        src.segs.push_back({reinterpret_cast<const uint8_t*>(sigs), n_sites * 8});
+        src.segs.push_back({reinterpret_cast<const uint8_t*>(slice_masks), n_slices * 8});
+        uint64_t base = 0;
+        const uint64_t valid = seq_len >= 64 ? ~0ull : ((1ull << seq_len) - 1);
+        for (uint64_t s = 0; s < n_slices; s++) {
+            const uint64_t w = static_cast<uint64_t>(__builtin_popcountll(slice_masks[s] & valid));
+            ISSL_REQUIRE(w <= 13, ISSL_ERR_UNSUPPORTED, "slice wider than 13 positions");
+            const uint64_t nb = 1ull << (2 * w);
+            src.segs.push_back({reinterpret_cast<const uint8_t*>(list_sizes + base), nb * 8});
+            src.segs.push_back({reinterpret_cast<const uint8_t*>(lists + s * n_sites), n_sites * 8});
+            base += nb;
+        }
+        auto ix = std::make_unique<issl_index>();
+        issl::load_stream(ix.get(), src, device);
+        *out = ix.release();
+    });
+}
+
+int issl_build(const uint64_t* sigs, const uint32_t* occ, uint64_t n_sites, const uint64_t* slice_masks,
+               uint64_t n_slices, int device, issl_index** out) {
+    return guarded([&] {
+        ISSL_REQUIRE(out && slice_masks && (n_sites == 0 || (sigs && occ)), ISSL_ERR_ARG, "issl_build: null argument");
+        *out = nullptr;
+        ISSL_CUDA(cudaSetDevice(device));
+        auto ix = std::make_unique<issl_index>();
+        ix->device = device;
+        ix->n_sites = n_sites;
+        ix->seq_len = issl::kSeqLen;
+        ix->n_slices = n_slices;
+        ix->masks.assign(slice_masks, slice_masks + n_slices);
+        ix->sigs.reserve(n_sites);
+        ix->occ.reserve(n_sites);
+        if (n_sites) {
+            ISSL_CUDA(cudaMemcpy(ix->sigs.p, sigs, n_sites * 8, cudaMemcpyHostToDevice));
+            ISSL_CUDA(cudaMemcpy(ix->occ.p, occ, n_sites * 4, cudaMemcpyHostToDevice));
+        }
+        cudaStream_t st;
+        ISSL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        try {
+            issl::build_from_device_sites(ix.get(), ix->sigs.p, ix->occ.p, st);
+        } catch (...) {
+            cudaStreamDestroy(st);
+            throw;
+        }
+        cudaStreamDestroy(st);
+        *out = ix.release();
+    });
+}
+
+int issl_close(issl_index* index) {
+    return guarded([&] {
+        if (!index) return;
+        cudaSetDevice(index->device);
+        delete index;
+    });
+}
+
+int issl_index_get_info(const issl_index* ix, issl_index_info* out) {
+    return guarded([&] {
+        ISSL_REQUIRE(ix && out, ISSL_ERR_ARG, "issl_index_get_info: null argument");
+        out->n_sites = ix->n_sites;
+        out->seq_len = ix->seq_len;
+        out->n_slices = ix->n_slices;
+        out->n_buckets = ix->n_buckets;
+        out->device_bytes = ix->sigs.bytes() + ix->occ.bytes() + ix->ids.bytes() + ix->resid.bytes() +
+                            ix->offsets.bytes() + ix->d_geom.bytes();
+        out->device = ix->device;
+        int mn = 64, mx = 0;
+        for (auto& g : ix->geom) {
+            mn = std::min<int>(mn, g.width);
+            mx = std::max<int>(mx, g.width);
+        }
+        out->min_width = mn;
+        out->max_width = mx;
+    });
+}
+
+int issl_export(const issl_index* ix, uint64_t* sigs, uint64_t* slice_masks, uint64_t* list_sizes, uint64_t* lists) {
+    return guarded([&] {
+        ISSL_REQUIRE(ix, ISSL_ERR_ARG, "issl_export: null index");
+        ISSL_CUDA(cudaSetDevice(ix->device));
+        if (sigs && ix->n_sites) ISSL_CUDA(cudaMemcpy(sigs, ix->sigs.p, ix->n_sites * 8, cudaMemcpyDeviceToHost));
+        if (slice_masks) std::memcpy(slice_masks, ix->masks.data(), ix->n_slices * 8);
+        if (list_sizes) {
+            auto sz = issl::export_sizes(ix);
+            std::memcpy(list_sizes, sz.data(), sz.size() * 8);
+        }
+        if (lists) {
+            cudaStream_t st;
+            ISSL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            for (uint64_t s = 0; s < ix->n_slices; s++) issl::export_slice_lists(ix, s, lists + s * ix->n_sites, st);
+            cudaStreamDestroy(st);
+        }
+    });
+}
+
+int issl_save(const issl_index* ix, const char* path) {
+    return guarded([&] {
+        ISSL_REQUIRE(ix && path, ISSL_ERR_ARG, "issl_save: null argument");
+        ISSL_CUDA(cudaSetDevice(ix->device));
+        FILE* fp = std::fopen(path, "wb");
+        ISSL_REQUIRE(fp, ISSL_ERR_IO, std::string("cannot create ") + path);
+        struct Closer {
+            FILE* f;
+            ~Closer() {
+                if (f) std::fclose(f);
+            }
+        } closer{fp};
+        auto put = [&](const void* p, size_t bytes) {
+            ISSL_REQUIRE(std::fwrite(p, 1, bytes, fp) == bytes, ISSL_ERR_IO, std::string("short write to ") + path);
+        };
+        const uint64_t hdr[3] = {ix->n_sites, ix->seq_len, ix->n_slices};
+        put(hdr, sizeof hdr);
+        std::vector<uint64_t> buf(ix->n_sites);
+        if (ix->n_sites) ISSL_CUDA(cudaMemcpy(buf.data(), ix->sigs.p, ix->n_sites * 8, cudaMemcpyDeviceToHost));
+        put(buf.data(), ix->n_sites * 8);
+        put(ix->masks.data(), ix->n_slices * 8);
+        auto sizes = issl::export_sizes(ix);
+        cudaStream_t st;
+        ISSL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        uint64_t base = 0;
+        for (uint64_t s = 0; s < ix->n_slices; s++) {
+            const uint64_t nb = 1ull << (2 * ix->geom[s].width);
+            put(sizes.data() + base, nb * 8);
+            issl::export_slice_lists(ix, s, buf.data(), st);
+            put(buf.data(), ix->n_sites * 8);
+            base += nb;
+        }
+        cudaStreamDestroy(st);
+        ISSL_REQUIRE(std::fclose(fp) == 0, ISSL_ERR_IO, std::string("cannot close ") + path);
+        closer.f = nullptr;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,152 @@
+// Internal declarations of the issl_b200 library (not part of the public C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "issl_b200.h"
+
+namespace issl {
+
+constexpr int kSeqLen = 20;     // protospacer length scored by the reference (20 nt)
+constexpr int kMaxSlices = 64;  // slices per index supported by the device tables
+constexpr int kMaxDist = 4;     // the reference's fixed mismatch bound (ISSLScoringModule.cpp:292)
+
+// ---- errors ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+void set_last_error(const std::string& msg);
+
+#define ISSL_CUDA(expr)                                                                         \
+    do {                                                                                        \
+        cudaError_t e_ = (expr);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            throw ::issl::Error(e_ == cudaErrorMemoryAllocation ? ISSL_ERR_NOMEM : ISSL_ERR_CUDA, \
+                                std::string(#expr) + ": " + cudaGetErrorString(e_));            \
+    } while (0)
+
+#define ISSL_REQUIRE(cond, code, msg)                   \
+    do {                                                \
+        if (!(cond)) throw ::issl::Error((code), (msg)); \
+    } while (0)
+
+// Runs f, converting exceptions into a status code + thread-local message.
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return ISSL_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return ISSL_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return ISSL_ERR_CUDA;
+    }
+}
+
+// ---- device memory ---------------------------------------------------------------------
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    // (re)allocates when the capacity is short; contents are not preserved
+    void reserve(size_t count) {
+        if (count <= n && p) return;
+        release();
+        size_t bytes = (count ? count : 1) * sizeof(T);
+        ISSL_CUDA(cudaMalloc(reinterpret_cast<void**>(&p), bytes));
+        n = count;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---- slice geometry ----------------------------------------------------------------------
+// Per-slice constants. A slice is a set of `width` protospacer positions; the key of a
+// signature is the 2-bit bases at those positions packed in ascending position order
+// (ISSLScoringModule.cpp:235-239). The residual is the bases at the other positions packed
+// the same way; it is what the scan compares, since the key positions match by construction.
+struct SliceGeom {
+    uint32_t pmask;       // 20-bit position mask
+    uint32_t bbase;       // first global bucket id of this slice (sum of 4^w of earlier slices)
+    uint8_t width;        // positions in the slice
+    uint8_t rwidth;       // positions outside the slice (20 - width)
+    uint8_t pos[kSeqLen]; // slice positions, ascending
+    uint8_t rpos[kSeqLen];// residual positions, ascending
+};
+
+std::vector<SliceGeom> make_geometry(const std::vector<uint64_t>& masks, uint64_t seq_len);
+
+// ---- the resident index ------------------------------------------------------------------
+struct Workspace;
+
+struct IndexView {  // POD view handed to kernels
+    const uint64_t* sigs;     // N packed signatures
+    const uint32_t* occ;      // N occurrence counts (one per site)
+    const uint32_t* ids;      // S*N site ids in list order (slice-major)
+    const uint32_t* resid;    // S*N residual codes in list order (+4 padding entries)
+    const uint64_t* offsets;  // G+1 bucket starts in global entry numbering: s*N + position
+    const SliceGeom* geom;    // S slice descriptors
+    uint64_t n_sites;
+    uint32_t n_slices;
+    uint32_t n_buckets;       // sum of 4^w
+};
+
+}  // namespace issl
+
+struct issl_index {
+    int device = 0;
+    uint64_t n_sites = 0, seq_len = 20, n_slices = 0, n_buckets = 0;
+    std::vector<uint64_t> masks;
+    std::vector<issl::SliceGeom> geom;
+    issl::DevBuf<uint64_t> sigs;
+    issl::DevBuf<uint32_t> occ, ids, resid;
+    issl::DevBuf<uint64_t> offsets;  // n_buckets + 1 global bucket starts
+    issl::DevBuf<issl::SliceGeom> d_geom;
+    std::unique_ptr<issl::Workspace> ws;
+    issl_score_stats stats{};
+    issl::IndexView view() const;
+    issl_index();  // defined where Workspace is complete
+    ~issl_index();
+};
+
+namespace issl {
+
+// builders (index.cu)
+void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint32_t* d_occ,
+                             cudaStream_t st);
+
+// radix sort (radix_sort.cu): stable LSD sort of (key, value) pairs on the low `bits` bits.
+size_t radix_sort_temp_bytes(size_t n, bool wide_keys);
+void radix_sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32_t* vals_tmp,
+                          size_t n, int bits, void* temp, size_t temp_bytes, cudaStream_t st,
+                          uint32_t** keys_out, uint32_t** vals_out);
+void radix_sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp,
+                          size_t n, int bits, void* temp, size_t temp_bytes, cudaStream_t st,
+                          uint64_t** keys_out, uint32_t** vals_out);
+
+// tables (tables.cpp)
+const std::vector<double>& mit_rank_table();   // 6195 entries indexed by subset rank
+const double* cfd_pos_table();
+const double* cfd_pam_table();
+
+}  // namespace issl

@@ -1,0 +1,56 @@
+"""Shared fixtures. GPU tests are marked `gpu`; everything else runs on CPU."""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(REPO, "tests", "golden")
+for p in (REPO, os.path.join(REPO, "oracle"), GOLDEN):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (runs the native CUDA path)")
+
+
+@pytest.fixture(scope="session")
+def penalties():
+    pen = json.load(open(os.path.join(GOLDEN, "penalties.json")))
+    masks = np.array([k for k, _ in pen["mit"]], np.uint64)
+    vals = np.array([float.fromhex(v) for _, v in pen["mit"]])
+    pos = np.array([float.fromhex(v) for v in pen["cfd_pos"]])
+    pam = np.array([float.fromhex(v) for v in pen["cfd_pam"]])
+    return {"mit_masks": masks, "mit_vals": vals, "cfd_pos": pos, "cfd_pam": pam, "raw": pen}
+
+
+@pytest.fixture(scope="session")
+def oracle(penalties):
+    import pyoracle
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle")], check=True)
+    pyoracle.set_cfd_tables(penalties["cfd_pos"], penalties["cfd_pam"])
+    return pyoracle
+
+
+@pytest.fixture(scope="session")
+def native():
+    from cracklingplusplus_gpu_b200 import build
+    build.build()
+    import cracklingplusplus_gpu_b200 as pkg
+    pkg.lib()
+    return pkg
+
+
+def load_case(name):
+    z = np.load(os.path.join(GOLDEN, f"case_{name}.npz"))
+    meta = json.loads(str(z["meta"]))
+    return z, meta
+
+
+CASE_NAMES = ["c0_small", "c1_small", "c2_small", "c4_small"]
