@@ -61,8 +61,8 @@ WORKLOAD = {
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--sites", type=int, default=None, help="override the site count (smaller runs)")
     ap.add_argument("--queries", type=int, default=None)
@@ -220,15 +220,16 @@ def run_ours(args):
                         d_code.data_ptr(), d_cnt.data_ptr(), d_dist.data_ptr(), stream.cuda_stream)
 
     # ---- device-resident throughput -------------------------------------------------------
-    for _ in range(args.warmup):
-        step_device()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
     scan_ms, scan_bytes, launches = [], [], 0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
+    with ClockSampler(local) as clocks:  # sampling starts before the warm-up (also under load)
+        for _ in range(args.warmup):
+            step_device()
         torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("timed_device")
         ev0.record(stream)
         for _ in range(args.steps):
             step_device()
@@ -238,6 +239,7 @@ def run_ours(args):
             launches += st.launches
         ev1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
     ms = ev0.elapsed_time(ev1)
     if world > 1:
         t = torch.tensor([ms], device=dev, dtype=torch.float64)

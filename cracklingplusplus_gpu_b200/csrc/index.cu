@@ -4,13 +4,16 @@
 //   sigs    [N]      u64  2-bit packed site signatures (the file's offtargets array)
 //   occ     [N]      u32  occurrence count per site (the high word of every list entry)
 //   ids     [S*N]    u32  site id per list entry (the low word of every list entry)
-//   resid   [S*N+4]  u32  residual code per list entry: the site's bases outside the slice
+//   rbits   [...]    u32  residual codes (the site's bases outside the slice), bit-sliced in
+//                         blocks of 32 list positions, one word per residual bit
+//   srec    [N]      16 B site record (signature, occurrences): the one random read per scored hit
 //   offsets [G+1]    u64  bucket starts in global entry numbering (slice s, position j -> s*N + j);
 //                         buckets are numbered slice by slice, so off[g+1] - off[g] is always the
 //                         size of bucket g, across slice boundaries too
 // The reference stores (occ << 32) | id per entry and gathers offtargets[id] for every entry it
-// scans (ISSLScoringModule.cpp:248-286). Here the scan streams resid only (4 bytes per entry)
-// because the slice positions of every entry in a bucket equal the query's by construction.
+// scans (ISSLScoringModule.cpp:248-286). Here the scan streams rbits only (2 * rwidth bits per
+// entry: 3 bytes for 8-nt slices) because the slice positions of every entry in a bucket equal
+// the query's by construction; bit-slicing lets one lane compare a guide with 32 entries at a time.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,7 +33,7 @@ thread_local std::string g_last_error;
 }
 void set_last_error(const std::string& m) { g_last_error = m; }
 
-std::vector<SliceGeom> make_geometry(const std::vector<uint64_t>& masks, uint64_t seq_len) {
+std::vector<SliceGeom> make_geometry(const std::vector<uint64_t>& masks, uint64_t seq_len, uint64_t n_sites) {
     ISSL_REQUIRE(seq_len >= 1 && seq_len <= kSeqLen, ISSL_ERR_UNSUPPORTED,
                  "only indexes of 20-nt (or shorter) sites are supported, got seqLength " +
                      std::to_string(seq_len));
@@ -38,7 +41,7 @@ std::vector<SliceGeom> make_geometry(const std::vector<uint64_t>& masks, uint64_
                  "slice count must be 1.." + std::to_string(kMaxSlices) + ", got " +
                      std::to_string(masks.size()));
     std::vector<SliceGeom> geom(masks.size());
-    uint64_t bbase = 0;
+    uint64_t bbase = 0, wbase = 0;
     const uint64_t valid = (1ull << seq_len) - 1;
     for (size_t s = 0; s < masks.size(); s++) {
         SliceGeom& g = geom[s];
@@ -57,12 +60,21 @@ std::vector<SliceGeom> make_geometry(const std::vector<uint64_t>& masks, uint64_
                          "; supported widths are 4..13 positions");
         g.width = static_cast<uint8_t>(w);
         g.rwidth = static_cast<uint8_t>(r);
+        g.wpb = static_cast<uint8_t>(2 * r + 1);
+        g.wbase = wbase;
+        wbase += blocks_per_slice(n_sites) * g.wpb;
         g.bbase = static_cast<uint32_t>(bbase);
         bbase += 1ull << (2 * w);
         ISSL_REQUIRE(bbase + masks.size() + 1 < (1ull << 32), ISSL_ERR_UNSUPPORTED,
                      "too many buckets over all slices");
     }
     return geom;
+}
+
+uint64_t bitsliced_words(const std::vector<SliceGeom>& geom, uint64_t n_sites) {
+    uint64_t w = 0;
+    for (auto& g : geom) w += blocks_per_slice(n_sites) * g.wpb;
+    return w;
 }
 
 namespace {
@@ -87,11 +99,25 @@ __global__ void k_offsets_from_sorted(const uint32_t* __restrict__ keys, uint64_
     }
 }
 
-__global__ void k_resid(const uint32_t* __restrict__ ids, const uint64_t* __restrict__ sigs, uint64_t n,
-                        SliceGeom g, uint32_t* __restrict__ resid) {
-    for (uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; j < n;
-         j += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        resid[j] = slice_residual(sigs[ids[j]], g);
+// Bit-sliced residual codes of one slice: a warp per block of 32 list positions; lane e holds the
+// residual code of entry e and a ballot per bit collects word j = bit j of the 32 codes.
+__global__ void k_rbits(const uint32_t* __restrict__ ids, const uint64_t* __restrict__ sigs, uint64_t n,
+                        SliceGeom g, uint32_t* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nblk = blocks_per_slice(n);
+    for (uint64_t b = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5; b < nblk;
+         b += (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5) {
+        const uint64_t pos = b * 32 + lane;
+        const uint32_t r = pos < n ? slice_residual(sigs[ids[pos]], g) : 0u;
+        uint32_t mine = 0;
+        const int nbits = 2 * g.rwidth;  // data words; word nbits is the zero padding word
+        for (int j = 0; j < nbits; j++) {
+            const uint32_t w = __ballot_sync(0xffffffffu, (r >> j) & 1u);
+            if (lane == j) mine = w;
+        }
+        if (lane < nbits) out[g.wbase + b * g.wpb + lane] = mine;
+        if (lane == 0) out[g.wbase + b * g.wpb + nbits] = 0u;
+    }
 }
 
 // bucket_of[j] for every list position j of one slice (off: the slice's nb+1 global starts)
@@ -131,6 +157,13 @@ __global__ void k_split_entries(const uint64_t* __restrict__ entries, uint64_t j
             atomicOr(flags, kOccMismatch);
         if (slice_key(sigs[id], g) != bucket_of[j]) atomicOr(flags, kWrongBucket);
     }
+}
+
+__global__ void k_site_records(const uint64_t* __restrict__ sigs, const uint32_t* __restrict__ occ, uint64_t n,
+                               uint4* __restrict__ out) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        out[i] = make_uint4(static_cast<uint32_t>(sigs[i]), static_cast<uint32_t>(sigs[i] >> 32), occ[i], 0u);
 }
 
 __global__ void k_join_entries(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ occ, uint64_t cnt,
@@ -252,16 +285,15 @@ void load_stream(issl_index* ix, Source& src, int device) {
     }
     ix->masks.resize(S);
     src.read(ix->masks.data(), S * 8, "reading slice masks failed");
-    ix->geom = make_geometry(ix->masks, ix->seq_len);
+    ix->geom = make_geometry(ix->masks, ix->seq_len, N);
     ix->n_buckets = count_buckets(ix->geom);
     ix->d_geom.reserve(S);
     ISSL_CUDA(cudaMemcpyAsync(ix->d_geom.p, ix->geom.data(), S * sizeof(SliceGeom), cudaMemcpyHostToDevice, st));
 
     ix->occ.reserve(N);
     ix->ids.reserve(S * N);
-    ix->resid.reserve(S * N + 4);
+    ix->rbits.reserve(bitsliced_words(ix->geom, N) + 4);
     ix->offsets.reserve(ix->n_buckets + 1);
-    ISSL_CUDA(cudaMemsetAsync(ix->resid.p + S * N, 0, 16, st));
     DevBuf<uint32_t> seen, bucket_of, flags;
     seen.reserve(N / 32 + 1);
     bucket_of.reserve(N);
@@ -302,7 +334,8 @@ void load_stream(issl_index* ix, Source& src, int device) {
             ISSL_CUDA(cudaEventRecord(stg.done[b], st));
             j += cnt;
         }
-        k_resid<<<grid_for(N), 256, 0, st>>>(ix->ids.p + s * N, ix->sigs.p, N, g, ix->resid.p + s * N);
+        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(ix->ids.p + s * N, ix->sigs.p, N, g,
+                                                                    ix->rbits.p);
         ISSL_CUDA(cudaGetLastError());
         uint32_t f = 0;
         ISSL_CUDA(cudaMemcpyAsync(&f, flags.p, 4, cudaMemcpyDeviceToHost, st));
@@ -315,6 +348,9 @@ void load_stream(issl_index* ix, Source& src, int device) {
         ISSL_REQUIRE(!(f & kWrongBucket), ISSL_ERR_FORMAT, where + "a site is listed under a bucket other than its key");
         bbase += nb;
     }
+    ix->srec.reserve(N);
+    k_site_records<<<grid_for(N), 256, 0, st>>>(ix->sigs.p, ix->occ.p, N, ix->srec.p);
+    ISSL_CUDA(cudaGetLastError());
     ISSL_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -323,7 +359,7 @@ void load_stream(issl_index* ix, Source& src, int device) {
 void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint32_t* d_occ, cudaStream_t st) {
     const uint64_t N = ix->n_sites, S = ix->n_slices;
     ISSL_REQUIRE(N < (1ull << 32), ISSL_ERR_UNSUPPORTED, "2^32 or more sites");
-    ix->geom = make_geometry(ix->masks, ix->seq_len);
+    ix->geom = make_geometry(ix->masks, ix->seq_len, N);
     ix->n_buckets = count_buckets(ix->geom);
     if (ix->sigs.p != d_sigs) {
         ix->sigs.reserve(N);
@@ -336,9 +372,8 @@ void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint3
     ix->d_geom.reserve(S);
     ISSL_CUDA(cudaMemcpyAsync(ix->d_geom.p, ix->geom.data(), S * sizeof(SliceGeom), cudaMemcpyHostToDevice, st));
     ix->ids.reserve(S * N);
-    ix->resid.reserve(S * N + 4);
+    ix->rbits.reserve(bitsliced_words(ix->geom, N) + 4);
     ix->offsets.reserve(ix->n_buckets + 1);
-    ISSL_CUDA(cudaMemsetAsync(ix->resid.p + S * N, 0, 16, st));
     DevBuf<uint32_t> keys, vals, keys2, vals2;
     DevBuf<uint8_t> temp;
     keys.reserve(N);
@@ -357,10 +392,14 @@ void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint3
         radix_sort_pairs_u32(keys.p, vals.p, keys2.p, vals2.p, N, 2 * g.width, temp.p, tb, st, &ko, &vo);
         if (N) ISSL_CUDA(cudaMemcpyAsync(ix->ids.p + s * N, vo, N * 4, cudaMemcpyDeviceToDevice, st));
         k_offsets_from_sorted<<<grid_for(N + 1), 256, 0, st>>>(ko, N, nb, s * N, ix->offsets.p + bbase);
-        k_resid<<<grid_for(N), 256, 0, st>>>(ix->ids.p + s * N, ix->sigs.p, N, g, ix->resid.p + s * N);
+        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(ix->ids.p + s * N, ix->sigs.p, N, g,
+                                                                    ix->rbits.p);
         ISSL_CUDA(cudaGetLastError());
         bbase += nb;
     }
+    ix->srec.reserve(N);
+    k_site_records<<<grid_for(N), 256, 0, st>>>(ix->sigs.p, ix->occ.p, N, ix->srec.p);
+    ISSL_CUDA(cudaGetLastError());
     ISSL_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -391,7 +430,8 @@ issl::IndexView issl_index::view() const {
     v.sigs = sigs.p;
     v.occ = occ.p;
     v.ids = ids.p;
-    v.resid = resid.p;
+    v.rbits = rbits.p;
+    v.srec = srec.p;
     v.offsets = offsets.p;
     v.geom = d_geom.p;
     v.n_sites = n_sites;
@@ -496,7 +536,7 @@ int issl_index_get_info(const issl_index* ix, issl_index_info* out) {
         out->seq_len = ix->seq_len;
         out->n_slices = ix->n_slices;
         out->n_buckets = ix->n_buckets;
-        out->device_bytes = ix->sigs.bytes() + ix->occ.bytes() + ix->ids.bytes() + ix->resid.bytes() +
+        out->device_bytes = ix->sigs.bytes() + ix->occ.bytes() + ix->ids.bytes() + ix->rbits.bytes() + ix->srec.bytes() +
                             ix->offsets.bytes() + ix->d_geom.bytes();
         out->device = ix->device;
         int mn = 64, mx = 0;

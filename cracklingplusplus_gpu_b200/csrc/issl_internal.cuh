@@ -85,16 +85,29 @@ struct DevBuf {
 // signature is the 2-bit bases at those positions packed in ascending position order
 // (ISSLScoringModule.cpp:235-239). The residual is the bases at the other positions packed
 // the same way; it is what the scan compares, since the key positions match by construction.
+//
+// The residual codes of a slice are stored bit-transposed ("bit-sliced") in blocks of 32
+// consecutive list positions: word j of a block holds bit j of the residual code of each of the
+// block's 32 entries (entry e at bit e). A block has wpb = 2 * rwidth + 1 words (the last one is
+// zero padding): an odd block stride puts the 32 blocks of a staged chunk in 32 different shared
+// memory banks, so lane l reading word j of block l never conflicts with another lane.
 struct SliceGeom {
+    uint64_t wbase;       // first word of this slice's blocks in the bit-sliced array
     uint32_t pmask;       // 20-bit position mask
     uint32_t bbase;       // first global bucket id of this slice (sum of 4^w of earlier slices)
     uint8_t width;        // positions in the slice
     uint8_t rwidth;       // positions outside the slice (20 - width)
+    uint8_t wpb;          // words per block of 32 entries
+    uint8_t pad;
     uint8_t pos[kSeqLen]; // slice positions, ascending
     uint8_t rpos[kSeqLen];// residual positions, ascending
 };
 
-std::vector<SliceGeom> make_geometry(const std::vector<uint64_t>& masks, uint64_t seq_len);
+constexpr int kBlockEntries = 32;
+__host__ __device__ inline uint64_t blocks_per_slice(uint64_t n_sites) { return (n_sites + 31) / 32; }
+
+std::vector<SliceGeom> make_geometry(const std::vector<uint64_t>& masks, uint64_t seq_len, uint64_t n_sites);
+uint64_t bitsliced_words(const std::vector<SliceGeom>& geom, uint64_t n_sites);
 
 // ---- the resident index ------------------------------------------------------------------
 struct Workspace;
@@ -103,7 +116,8 @@ struct IndexView {  // POD view handed to kernels
     const uint64_t* sigs;     // N packed signatures
     const uint32_t* occ;      // N occurrence counts (one per site)
     const uint32_t* ids;      // S*N site ids in list order (slice-major)
-    const uint32_t* resid;    // S*N residual codes in list order (+4 padding entries)
+    const uint32_t* rbits;    // bit-sliced residual codes (see SliceGeom)
+    const uint4* srec;        // N site records (signature low, signature high, occurrences, 0)
     const uint64_t* offsets;  // G+1 bucket starts in global entry numbering: s*N + position
     const SliceGeom* geom;    // S slice descriptors
     uint64_t n_sites;
@@ -119,8 +133,9 @@ struct issl_index {
     std::vector<uint64_t> masks;
     std::vector<issl::SliceGeom> geom;
     issl::DevBuf<uint64_t> sigs;
-    issl::DevBuf<uint32_t> occ, ids, resid;
+    issl::DevBuf<uint32_t> occ, ids, rbits;
     issl::DevBuf<uint64_t> offsets;  // n_buckets + 1 global bucket starts
+    issl::DevBuf<uint4> srec;        // per site: signature and occurrences in one 16-byte record
     issl::DevBuf<issl::SliceGeom> d_geom;
     std::unique_ptr<issl::Workspace> ws;
     issl_score_stats stats{};

@@ -22,41 +22,45 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
+#include "async_copy.cuh"
+#include "bitslice.cuh"
 #include "device_util.cuh"
 #include "issl_internal.cuh"
 #include "scan.cuh"
 
 namespace issl {
 
-constexpr int kChunk = 512;        // entries per scan unit
+constexpr int kChunk = 1024;       // list positions per scan unit: 32 bit-sliced blocks of 32
 constexpr int kGroup = 32;         // guides per scan unit
 constexpr int kWarpHits = 256;     // guides with more hits are scored by a whole block
-constexpr int kScanWarps = 8;      // warps per scan block
-constexpr int kHitBuf = 64;        // per-warp staging of hits before one global reservation
+constexpr int kScanWarps = 4;      // warps per scan block
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 
 struct UnitDesc {   // 16 bytes
-    uint64_t cb;    // first global entry (s * N + list position)
+    uint32_t p0;    // first list position of the unit within its slice
     uint32_t qbeg;  // first probe slot of the unit's guides
-    uint16_t len;   // entries in the unit (<= kChunk)
+    uint16_t len;   // list positions in the unit (<= kChunk, inside one aligned kChunk block)
     uint8_t qn;     // guides in the unit (<= kGroup)
     uint8_t s;      // slice
+    uint32_t pad;
 };
 
 struct Counters {
     uint64_t bucket_total;  // hi: units, lo: probes into non-empty buckets
     uint32_t n_units;       // min(units, capacity)
-    uint32_t n_hits;        // owned hits appended (may exceed capacity -> overflow)
-    uint32_t hit_total;     // sum of per-guide hits (scan total)
+    uint32_t n_cand;        // hit slots reserved by the scan (may exceed capacity -> overflow)
+    uint32_t hit_total;     // owned hits: sum of per-guide hits (scan total)
     uint32_t n_big;         // guides deferred to the block scorer
-    uint32_t overflow;      // 1: units, 2: hits
+    uint32_t overflow;      // 1: units, 2: hits, 4: a bounded wait in the scan gave up
     uint32_t pad;
     uint64_t distinct;
     uint64_t buckets;       // distinct buckets probed
-    uint64_t entries;       // entries streamed by the scan
+    uint64_t entries;       // entries compared by the scan (per guide group)
+    uint64_t rbytes;        // bit-sliced bytes the scan copies
 };
 
 struct Tables {  // device copies of the penalty tables
@@ -75,23 +79,62 @@ struct ScoreParams {
     int want_distinct;
 };
 
+constexpr int kStages = 3;
+constexpr int kStageQr = kGroup + 2;     // (guide, residual) pairs per stage + alignment slack
+constexpr uint32_t kCandSlab = 256;
+constexpr uint32_t kDeadCand = 0xFFFFFFFFu;  // guide field of an unused or rejected candidate slot
+constexpr int kGuideBits = 26;               // candidate records pack guide | slice << 26
+constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 1.965 GHz
+
+struct StageMeta {
+    uint32_t p0;   // first list position of the unit
+    uint32_t len;  // list positions in the unit
+    uint32_t b0;   // first block of the unit
+    uint32_t nb;   // blocks in the unit
+    uint32_t qoff; // offset of the unit's first guide in the staged pairs
+    uint32_t qn;   // guides in the unit
+    uint32_t s;    // slice
+    uint32_t delta;// words between the 16-byte aligned copy start and the unit's first block
+};
+
+// per-warp shared memory, sized at launch for the widest block of the index
+struct WarpLayout {
+    uint32_t stage_words;  // 32 blocks x words per block (largest slice)
+    uint32_t qr_off, qm_off, meta_off, bar_off, bytes;
+};
+
+__host__ __device__ inline WarpLayout warp_layout(uint32_t max_wpb) {
+    WarpLayout L;
+    L.stage_words = (32u * max_wpb + 3u + 3u) & ~3u;  // 32 blocks + alignment slack, 16-byte multiple
+    L.qr_off = kStages * L.stage_words * 4u;                 // 16-byte aligned (stage_words % 4 == 0)
+    L.qm_off = L.qr_off + kStages * kStageQr * 8u;
+    L.meta_off = L.qm_off + 32u * 4u;
+    L.bar_off = L.meta_off + kStages * static_cast<uint32_t>(sizeof(StageMeta));
+    L.bytes = (L.bar_off + kStages * 8u + 15u) & ~15u;
+    return L;
+}
+
 }  // namespace issl
 
 struct issl::Workspace {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    size_t q_cap = 0, unit_cap = 0, hit_cap = 0;
+    size_t q_cap = 0, unit_cap = 0, cand_cap = 0;
     uint64_t g_cap = 0;
     int scan_blocks = 0;
+    int scan_rw = 0;  // residual width the scan is specialised for (0: mixed)
+    WarpLayout scan_layout{};
+    int scan_smem = 0;
     bool zero_state_ok = false;  // bucket_cnt / qhits are all zero between calls
     DevBuf<uint64_t> qsig;
     DevBuf<char> ascii;
     size_t ascii_cap = 0;
-    DevBuf<uint32_t> probe_gb, probe_q, probe_rq;
+    DevBuf<uint32_t> probe_gb;
+    DevBuf<uint64_t> probe_qr;  // per probe slot: guide | residual << 32 (+2 padding)
     DevBuf<uint32_t> bucket_cnt, bucket_qstart;
     DevBuf<UnitDesc> units;
-    DevBuf<uint4> hits, seg;
+    DevBuf<uint4> cands, seg;  // candidate slots; owned hits grouped per guide
     DevBuf<uint32_t> qhits, qhoff, big;
     DevBuf<uint32_t> bitmap;
     DevBuf<Counters> counters;
@@ -155,11 +198,14 @@ __global__ void k_probe_count(IndexView ix, const uint64_t* __restrict__ qsig, u
 struct BucketLoad {
     const uint32_t* cnt;
     const uint64_t* off;
+    uint64_t n_sites;
     __device__ uint64_t operator()(uint64_t g) const {
         const uint32_t c = cnt[g];
         if (!c) return 0;
-        const uint64_t size = off[g + 1] - off[g];
-        const uint64_t units = ((size + kChunk - 1) / kChunk) * ((c + kGroup - 1) / kGroup);
+        // chunks are aligned to kChunk list positions of the slice, so a unit never spans two
+        const uint64_t sb = (off[g] / n_sites) * n_sites;
+        const uint64_t chunks = (off[g + 1] - 1 - sb) / kChunk - (off[g] - sb) / kChunk + 1;
+        const uint64_t units = chunks * ((c + kGroup - 1) / kGroup);
         return (units << 32) | c;
     }
 };
@@ -176,20 +222,23 @@ struct BucketStore {
         const uint32_t c = static_cast<uint32_t>(inc) - static_cast<uint32_t>(ex);
         if (!c) return;
         const uint64_t u0 = ex >> 32, u1 = inc >> 32;
-        const uint64_t e0 = off[g], e1 = off[g + 1];
-        const uint32_t s = static_cast<uint32_t>(e0 / n_sites);
+        const uint32_t s = static_cast<uint32_t>(off[g] / n_sites);
+        const uint64_t e0 = off[g] - s * n_sites, e1 = off[g + 1] - s * n_sites;  // list positions
         const uint32_t ng = (c + kGroup - 1) / kGroup;
         uint64_t u = u0;
-        for (uint64_t cb = e0; cb < e1 && u < u1; cb += kChunk) {
-            const uint16_t len = static_cast<uint16_t>(e1 - cb < kChunk ? e1 - cb : kChunk);
+        for (uint64_t blk = e0 / kChunk; blk * kChunk < e1 && u < u1; blk++) {
+            const uint64_t cb = blk * kChunk > e0 ? blk * kChunk : e0;
+            const uint64_t ce = (blk + 1) * kChunk < e1 ? (blk + 1) * kChunk : e1;
+            const uint16_t len = static_cast<uint16_t>(ce - cb);
             for (uint32_t j = 0; j < ng; j++, u++) {
                 if (u >= unit_cap) return;
                 UnitDesc d;
-                d.cb = cb;
+                d.p0 = static_cast<uint32_t>(cb);
                 d.qbeg = static_cast<uint32_t>(ex) + j * kGroup;
                 d.len = len;
                 d.qn = static_cast<uint8_t>(c - j * kGroup < kGroup ? c - j * kGroup : kGroup);
                 d.s = static_cast<uint8_t>(s);
+                d.pad = 0;
                 units[u] = d;
             }
         }
@@ -199,22 +248,28 @@ struct BucketStore {
 // work counters for the roofline: distinct buckets scanned and entries streamed (a bucket's
 // entries are read once per group of up to kGroup guides)
 __global__ void k_bucket_stats(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off, uint64_t G,
-                               Counters* c) {
-    uint64_t buckets = 0, entries = 0;
+                               const SliceGeom* __restrict__ geom, uint64_t n_sites, Counters* c) {
+    uint64_t buckets = 0, entries = 0, bytes = 0;
     for (uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < G;
          g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint32_t k = cnt[g];
         if (!k) continue;
+        const uint64_t groups = (k + kGroup - 1) / kGroup;
+        const uint64_t s = off[g] / n_sites, p0 = off[g] - s * n_sites, p1 = off[g + 1] - s * n_sites;
         buckets++;
-        entries += (off[g + 1] - off[g]) * ((k + kGroup - 1) / kGroup);
+        entries += (p1 - p0) * groups;
+        // bit-sliced blocks copied: every block the bucket touches, once per guide group
+        bytes += ((p1 - 1) / 32 - p0 / 32 + 1) * geom[s].wpb * 4ull * groups;
     }
     for (int d = 16; d > 0; d >>= 1) {
         buckets += __shfl_down_sync(0xffffffffu, buckets, d);
         entries += __shfl_down_sync(0xffffffffu, entries, d);
+        bytes += __shfl_down_sync(0xffffffffu, bytes, d);
     }
     if ((threadIdx.x & 31) == 0 && buckets) {
         atomicAdd(reinterpret_cast<unsigned long long*>(&c->buckets), buckets);
         atomicAdd(reinterpret_cast<unsigned long long*>(&c->entries), entries);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&c->rbytes), bytes);
     }
 }
 
@@ -224,11 +279,10 @@ __global__ void k_units_finalize(Counters* c, uint64_t unit_cap) {
     if (u > unit_cap) atomicOr(&c->overflow, 1u);
 }
 
-// 3. guides grouped by bucket, with their residual codes
+// 3. guides grouped by bucket; each slot holds (guide index, guide residual code for the slice)
 __global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig, uint64_t n,
                                 const uint32_t* __restrict__ probe_gb, uint32_t* __restrict__ bucket_cnt,
-                                const uint32_t* __restrict__ qstart, uint32_t* __restrict__ probe_q,
-                                uint32_t* __restrict__ probe_rq) {
+                                const uint32_t* __restrict__ qstart, uint64_t* __restrict__ probe_qr) {
     __shared__ SliceGeom g[kMaxSlices];
     for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
     __syncthreads();
@@ -241,128 +295,281 @@ __global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig,
         const uint32_t s = static_cast<uint32_t>(p - q * S);
         // the decrement leaves bucket_cnt all zero for the next call
         const uint32_t slot = qstart[gb] + atomicSub(&bucket_cnt[gb], 1u) - 1u;
-        probe_q[slot] = static_cast<uint32_t>(q);
-        probe_rq[slot] = slice_residual(qsig[q], g[s]);
+        probe_qr[slot] = q | (static_cast<uint64_t>(slice_residual(qsig[q], g[s])) << 32);
     }
 }
 
 // ---------------------------------------------------------------------------------------------
 // 4. the scan
+//
+// A unit is up to 32 bit-sliced blocks of 32 list positions (kChunk = 1024 entries) and up to
+// kGroup guides. Each warp runs its own kStages-deep ring in shared memory: for unit t + kStages
+// it issues two bulk copies (cp.async.bulk, the TMA engine) -- the unit's blocks and its guides'
+// (index, residual) pairs -- completing on the stage's mbarrier, while it computes unit t from
+// the stage that has landed. Lane l takes block l: per guide it forms the mismatch word of every
+// residual position (32 entries at once), adds them with a carry-save tree and keeps the entries
+// within max_dist. Candidates (rare) are written, with their residual mismatch mask, to slabs
+// of the candidate buffer that the warp reserves kCandSlab at a time; k_cand_own then applies the
+// ownership rule to the masks with every lane busy and no memory gathers.
 struct ScanArgs {
-    const uint32_t* resid;
+    const uint32_t* rbits;
     const SliceGeom* geom;
     const UnitDesc* units;
-    const uint32_t* probe_q;
-    const uint32_t* probe_rq;
+    const uint64_t* probe_qr;
     Counters* counters;
-    uint4* hits;
-    uint32_t* qhits;
-    uint64_t n_sites;
-    uint32_t hit_cap;
+    uint4* cands;
     uint32_t n_slices;
+    uint32_t cand_cap;
     int max_dist;
+    WarpLayout L;
 };
 
-__device__ __forceinline__ uint4 ld_resid4(const uint32_t* p) {
-    return __ldg(reinterpret_cast<const uint4*>(p));
+struct ScanShared {  // per-block slice tables
+    uint64_t wbase[kMaxSlices];
+    uint8_t wpb[kMaxSlices], rw[kMaxSlices];
+};
+
+struct ScanCtx {  // per-warp state of the candidate slab
+    uint32_t cpos, cend;
+    bool full;
+};
+
+// Compares every guide of the unit with the lane's block (RW residual positions per entry).
+template <int RW>
+__device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb, const uint64_t* qr, uint32_t* qm,
+                                          const StageMeta& m, uint32_t wpb, int lane, ScanCtx& cx) {
+    constexpr int NW = 2 * RW;
+    constexpr int NV = (NW + 3) / 4;
+    const unsigned lt = (1u << lane) - 1u;
+    // this lane's block and the entries of it that belong to the unit
+    uint32_t d[NW];
+    uint32_t valid = 0;
+    const uint32_t bl = m.b0 + lane;
+    if (static_cast<uint32_t>(lane) < m.nb) {
+        const int lo = max(static_cast<int>(m.p0) - static_cast<int>(32 * bl), 0);
+        const int hi = min(static_cast<int>(m.p0 + m.len) - static_cast<int>(32 * bl), 32);
+        valid = (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
+    }
+    // odd block stride: the 32 lanes read 32 different banks. Words of lanes past the unit are
+    // stale but masked by `valid`.
+    const uint32_t* blk = rb + m.delta + lane * wpb;
+#pragma unroll
+    for (int j = 0; j < NW; j++) d[j] = blk[j];
+    const uint4* qm4 = reinterpret_cast<const uint4*>(qm);
+    for (uint32_t k = 0; k < m.qn; k++) {
+        const uint64_t g = qr[m.qoff + k];
+        const uint32_t rq = static_cast<uint32_t>(g >> 32);
+        __syncwarp();
+        if (lane < NW) qm[lane] = 0u - ((rq >> lane) & 1u);  // guide bit j spread to a word
+        __syncwarp();
+        // mismatch word of each residual position: guide masks come as 128-bit broadcast reads,
+        // two positions per read
+        uint32_t mm[RW];
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const uint4 w = qm4[v];
+            if (2 * v < RW) mm[2 * v] = (d[4 * v] ^ w.x) | (d[4 * v + 1] ^ w.y);
+            if (2 * v + 1 < RW) mm[2 * v + 1] = (d[4 * v + 2] ^ w.z) | (d[4 * v + 3] ^ w.w);
+        }
+        uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), a.max_dist) & valid;
+        // candidates are rare: one per lane per round, written to the warp's slab as
+        // (guide | slice << 26, list position, residual mismatch mask); k_cand_own applies the
+        // ownership rule to the mask
+        for (unsigned hm = __ballot_sync(0xffffffffu, cbits != 0); hm; hm = __ballot_sync(0xffffffffu, cbits != 0)) {
+            const uint32_t nh = __popc(hm);
+            if (cx.cpos + nh > cx.cend) {
+                // retire the rest of the slab, reserve a new one
+                for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
+                    if (i < a.cand_cap) a.cands[i] = make_uint4(kDeadCand, 0, 0, 0);
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&a.counters->n_cand, kCandSlab);
+                cx.cpos = __shfl_sync(0xffffffffu, base, 0);
+                cx.cend = cx.cpos + kCandSlab;
+                cx.full = cx.cend > a.cand_cap;
+            }
+            if (cbits) {
+                const int e = __ffs(cbits) - 1;
+                cbits &= cbits - 1;
+                uint32_t rm = 0;  // bit p: residual position p of entry e mismatches the guide
+#pragma unroll
+                for (int p = 0; p < RW; p++) rm |= ((mm[p] >> e) & 1u) << p;
+                if (!cx.full)
+                    a.cands[cx.cpos + __popc(hm & lt)] =
+                        make_uint4(static_cast<uint32_t>(g) | (m.s << kGuideBits), 32u * bl + e, rm, 0u);
+            }
+            cx.cpos += nh;
+        }
+    }
 }
 
+// RWFIX > 0: every slice of the index has RWFIX residual positions; 0: mixed widths
+template <int RWFIX>
 __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
-    __shared__ uint32_t s_pmask[kMaxSlices];
-    __shared__ uint8_t s_rpos[kMaxSlices][kSeqLen];
-    __shared__ uint4 s_buf[kScanWarps][kHitBuf];
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    __shared__ ScanShared sh;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const WarpLayout L = a.L;
+    uint8_t* wbase_ptr = smem_raw + static_cast<size_t>(warp) * L.bytes;
+    uint32_t* rb = reinterpret_cast<uint32_t*>(wbase_ptr);
+    uint64_t* qr = reinterpret_cast<uint64_t*>(wbase_ptr + L.qr_off);
+    uint32_t* qm = reinterpret_cast<uint32_t*>(wbase_ptr + L.qm_off);
+    StageMeta* meta = reinterpret_cast<StageMeta*>(wbase_ptr + L.meta_off);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(wbase_ptr + L.bar_off);
     for (int i = threadIdx.x; i < static_cast<int>(a.n_slices); i += blockDim.x) {
-        s_pmask[i] = a.geom[i].pmask;
-        for (int j = 0; j < kSeqLen; j++) s_rpos[i][j] = a.geom[i].rpos[j];
+        sh.wbase[i] = a.geom[i].wbase;
+        sh.wpb[i] = a.geom[i].wpb;
+        sh.rw[i] = a.geom[i].rwidth;
+    }
+    if (lane == 0) {
+        for (int st = 0; st < kStages; st++) mbar_init(&bar[st], 1);
+        fence_barrier_init();
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    const uint32_t n_units = a.counters->n_units;
-    const uint32_t gwarp = blockIdx.x * kScanWarps + warp;
-    const uint32_t nwarps = gridDim.x * kScanWarps;
-    uint32_t buffered = 0;
-    uint4* buf = s_buf[warp];
 
-    auto flush = [&]() {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&a.counters->n_hits, buffered);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        for (uint32_t i = lane; i < buffered; i += 32)
-            if (base + i < a.hit_cap) a.hits[base + i] = buf[i];
-        __syncwarp();
-        buffered = 0;
+    const uint32_t n_units = a.counters->n_units;
+    const uint32_t nwarps = gridDim.x * kScanWarps;
+    const uint32_t gw = blockIdx.x * kScanWarps + warp;
+    // this warp owns batches gw, gw + nwarps, ... of 32 consecutive units
+    const uint32_t n_batches = (n_units + 31) / 32;
+    const uint32_t my_batches = n_batches > gw ? (n_batches - gw + nwarps - 1) / nwarps : 0;
+    uint32_t T = 0;
+    if (my_batches) {
+        const uint32_t last = gw + (my_batches - 1) * nwarps;
+        T = (my_batches - 1) * 32 + min(32u, n_units - last * 32);
+    }
+    auto load_desc = [&](uint32_t bi) -> uint4 {
+        const uint32_t u = (gw + bi * nwarps) * 32 + lane;
+        return (bi < my_batches && u < n_units) ? __ldg(reinterpret_cast<const uint4*>(a.units) + u)
+                                                : make_uint4(0, 0, 0, 0);
+    };
+    uint32_t ba = 0;
+    uint4 dA = load_desc(0), dB = load_desc(1);
+
+    // issue the copies of unit t (all lanes call; lane 0 issues)
+    auto issue = [&](uint32_t t) {
+        if ((t >> 5) != ba) {
+            dA = dB;
+            ba++;
+            dB = load_desc(ba + 1);
+        }
+        const int src = t & 31;
+        const uint32_t p0 = __shfl_sync(0xffffffffu, dA.x, src), qbeg = __shfl_sync(0xffffffffu, dA.y, src);
+        const uint32_t dz = __shfl_sync(0xffffffffu, dA.z, src);
+        if (lane == 0) {
+            const int st = t % kStages;
+            const uint32_t len = dz & 0xFFFFu, qn = (dz >> 16) & 0xFFu, s = dz >> 24;
+            const uint32_t b0 = p0 / 32u, nb = (p0 + len - 1) / 32u - b0 + 1;  // <= 32: inside one chunk
+            const uint32_t wpb = sh.wpb[s];
+            // blocks are wpb (odd) words long: copy from the 16-byte boundary at or below the
+            // first block and skip the `delta` leading words in shared memory
+            const uint64_t w0 = sh.wbase[s] + static_cast<uint64_t>(b0) * wpb, wa = w0 & ~3ull;
+            const uint32_t delta = static_cast<uint32_t>(w0 - wa);
+            const uint32_t nwords = (delta + nb * wpb + 3u) & ~3u;
+            const uint32_t qa0 = qbeg & ~1u, qa1 = (qbeg + qn + 1) & ~1u;
+            StageMeta& m = meta[st];
+            m.p0 = p0;
+            m.len = len;
+            m.b0 = b0;
+            m.nb = nb;
+            m.qoff = qbeg - qa0;
+            m.qn = qn;
+            m.s = s;
+            m.delta = delta;
+            const uint32_t rbytes = nwords * 4u, qbytes = (qa1 - qa0) * 8u;
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&bar[st], rbytes + qbytes);
+            bulk_copy_g2s(rb + st * L.stage_words, a.rbits + wa, rbytes, &bar[st]);
+            bulk_copy_g2s(qr + st * kStageQr, a.probe_qr + qa0, qbytes, &bar[st]);
+        }
     };
 
-    for (uint32_t u = gwarp; u < n_units; u += nwarps) {
-        const UnitDesc d = a.units[u];
-        const uint32_t s = d.s;
-        uint32_t q = 0, rq = 0;
-        if (lane < d.qn) {
-            q = a.probe_q[d.qbeg + lane];
-            rq = a.probe_rq[d.qbeg + lane];
+    ScanCtx cx{0u, 0u, false};
+    const uint32_t pro = T < kStages ? T : kStages;
+    for (uint32_t t = 0; t < pro; t++) issue(t);
+    __syncwarp();
+
+    uint32_t t = 0;
+    bool failed = false;
+    for (; t < T; t++) {
+        const int st = t % kStages;
+        const bool ok = mbar_wait_bounded(&bar[st], (t / kStages) & 1u, kWaitCycles);
+        if (__any_sync(0xffffffffu, !ok)) {
+            failed = true;
+            break;
         }
-        const uint64_t cb = d.cb, ce = d.cb + d.len;
-        const uint64_t a0 = cb & ~3ull;
-        // issue every load of the unit before using any (kChunk / 128 + 1 vectors per lane)
-        constexpr int kVec = kChunk / 128 + 1;
-        uint4 v[kVec];
-#pragma unroll
-        for (int it = 0; it < kVec; it++) {
-            const uint64_t base = a0 + static_cast<uint64_t>(it) * 128 + 4 * lane;
-            v[it] = base < ce ? ld_resid4(a.resid + base) : make_uint4(0, 0, 0, 0);
+        const StageMeta m = meta[st];
+        const uint32_t wpb = sh.wpb[m.s];
+        const uint32_t* srb = rb + st * L.stage_words;
+        const uint64_t* sqr = qr + st * kStageQr;
+        if constexpr (RWFIX > 0) {
+            scan_unit<RWFIX>(a, srb, sqr, qm, m, wpb, lane, cx);
+        } else switch (sh.rw[m.s]) {  // uniform across the warp
+            case 12: scan_unit<12>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            case 10: scan_unit<10>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            case 16: scan_unit<16>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            case 15: scan_unit<15>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            case 14: scan_unit<14>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            case 13: scan_unit<13>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            case 11: scan_unit<11>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            case 9: scan_unit<9>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            case 8: scan_unit<8>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            default: scan_unit<7>(a, srb, sqr, qm, m, wpb, lane, cx); break;
         }
-        const uint64_t slice_base = static_cast<uint64_t>(s) * a.n_sites;
-        for (int k = 0; k < d.qn; k++) {
-            const uint32_t rqk = __shfl_sync(0xffffffffu, rq, k);
-            const uint32_t qk = __shfl_sync(0xffffffffu, q, k);
-#pragma unroll
-            for (int it = 0; it < kVec; it++) {
-                const uint64_t base = a0 + static_cast<uint64_t>(it) * 128 + 4 * lane;
-                const uint32_t r4[4] = {v[it].x, v[it].y, v[it].z, v[it].w};
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const uint32_t m = fold32(r4[e] ^ rqk);
-                    const uint64_t idx = base + e;
-                    const bool cand = __popc(m) <= a.max_dist && idx >= cb && idx < ce;
-                    const unsigned cm = __ballot_sync(0xffffffffu, cand);
-                    if (cm == 0) continue;
-                    bool own = false;
-                    if (cand) {
-                        // mismatch positions of the whole site: residual mismatches only (the
-                        // slice positions match by construction)
-                        uint32_t mism20 = 0, mm = m;
-                        while (mm) {
-                            const int b = __ffs(mm) - 1;
-                            mism20 |= 1u << s_rpos[s][b >> 1];
-                            mm &= mm - 1;
-                        }
-                        own = true;
-                        for (uint32_t t = 0; t < s; t++)
-                            if ((mism20 & s_pmask[t]) == 0) {
-                                own = false;
-                                break;
-                            }
-                    }
-                    const unsigned om = __ballot_sync(0xffffffffu, own);
-                    if (om == 0) continue;
-                    if (buffered + 32 > kHitBuf) flush();
-                    if (own) {
-                        buf[buffered + __popc(om & lt)] =
-                            make_uint4(qk, static_cast<uint32_t>(idx - slice_base), s, r4[e]);
-                        atomicAdd(&a.qhits[qk], 1u);
-                    }
-                    __syncwarp();
-                    buffered += __popc(om);
-                }
-            }
-        }
+        __syncwarp();  // every lane is done with stage st before it is refilled
+        if (t + kStages < T) issue(t + kStages);
     }
-    if (buffered) flush();
+    if (failed) {
+        // a copy did not land in time: report, then wait (bounded) for this warp's copies in flight
+        if (lane == 0) atomicOr(&a.counters->overflow, 4u);
+        for (uint32_t u = t; u < T && u < t + kStages; u++)
+            mbar_wait_bounded(&bar[u % kStages], (u / kStages) & 1u, kWaitCycles);
+    }
+    for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
+        if (i < a.cand_cap) a.cands[i] = make_uint4(kDeadCand, 0, 0, 0);
+}
+
+__global__ void k_cands_finalize(Counters* c, uint32_t cand_cap) {
+    if (c->n_cand > cand_cap) atomicOr(&c->overflow, 2u);
+}
+
+// 5. the ownership rule on the candidates: a site reached in slice s is counted only if no
+// earlier slice has all its positions matching, i.e. every earlier slice mask meets the
+// mismatch positions (the residual mismatch mask spread back to protospacer positions).
+// Rejected slots are marked dead; owned ones are counted per guide.
+__global__ void k_cand_own(uint4* __restrict__ cands, const Counters* c, IndexView ix, uint32_t* __restrict__ qhits) {
+    __shared__ uint32_t s_pmask[kMaxSlices];
+    __shared__ uint8_t s_rpos[kMaxSlices][kSeqLen];
+    for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) {
+        s_pmask[i] = ix.geom[i].pmask;
+        for (int j = 0; j < kSeqLen; j++) s_rpos[i][j] = ix.geom[i].rpos[j];
+    }
+    __syncthreads();
+    if (c->overflow) return;  // the host grows the buffers and reruns
+    const uint32_t n = c->n_cand;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint4 r = cands[i];
+        if (r.x == kDeadCand) continue;
+        const uint32_t s = r.x >> kGuideBits;
+        uint32_t mism20 = 0, mm = r.z;
+        while (mm) {
+            mism20 |= 1u << s_rpos[s][__ffs(mm) - 1];
+            mm &= mm - 1;
+        }
+        bool own = true;
+        for (uint32_t e = 0; e < s; e++)
+            if ((mism20 & s_pmask[e]) == 0) {
+                own = false;  // an earlier slice reaches this site
+                break;
+            }
+        if (own)
+            atomicAdd(&qhits[r.x & ((1u << kGuideBits) - 1u)], 1u);
+        else
+            cands[i].x = kDeadCand;
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
-// 5/6. hits grouped per guide
+// 6. hits grouped per guide
 struct LoadQhits {
     const uint32_t* p;
     __device__ uint32_t operator()(uint64_t i) const { return p[i]; }
@@ -372,18 +579,20 @@ struct StoreQoff {
     __device__ void operator()(uint64_t i, uint32_t ex, uint32_t) const { p[i] = ex; }
 };
 
-__global__ void k_hit_scatter(const uint4* __restrict__ hits, const Counters* c, uint32_t hit_cap,
-                              uint32_t* __restrict__ qhits, const uint32_t* __restrict__ qhoff,
-                              const uint32_t* __restrict__ ids, uint64_t n_sites, uint4* __restrict__ seg) {
-    // on overflow the per-guide offsets count hits that were not stored: skip, the host reruns
-    if (c->n_hits > hit_cap || c->overflow) return;
-    const uint32_t n = c->n_hits;
+__global__ void k_hit_scatter(const uint4* __restrict__ cands, const Counters* c, uint32_t* __restrict__ qhits,
+                              const uint32_t* __restrict__ qhoff, const uint32_t* __restrict__ ids, uint64_t n_sites,
+                              uint4* __restrict__ seg) {
+    if (c->overflow) return;
+    const uint32_t n = c->n_cand;
     for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x) {
-        const uint4 r = hits[h];
-        const uint32_t q = r.x;
+        const uint4 r = cands[h];
+        if (r.x == kDeadCand) continue;
+        const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
+        // the decrement leaves qhits all zero for the next call
         const uint32_t slot = qhoff[q] + atomicSub(&qhits[q], 1u) - 1u;
-        // seg record: (list position, slice, residual code, site id)
-        seg[slot] = make_uint4(r.y, r.z, r.w, ids[static_cast<uint64_t>(r.z) * n_sites + r.y]);
+        // seg record: (list position, slice, residual mismatch mask, site id)
+        const uint32_t sl = r.x >> kGuideBits;
+        seg[slot] = make_uint4(r.y, sl, r.z, ids[static_cast<uint64_t>(sl) * n_sites + r.y]);
     }
 }
 
@@ -391,13 +600,6 @@ __global__ void k_hit_scatter(const uint4* __restrict__ hits, const Counters* c,
 // 7. scoring of one guide's hits in the reference's visiting order
 __device__ __forceinline__ uint64_t order_key(const uint4& r) {
     return (static_cast<uint64_t>(r.y) << 32) | r.x;  // slice, then list position
-}
-
-__device__ __forceinline__ uint64_t site_signature(uint64_t q, const SliceGeom& g, uint32_t r) {
-    uint64_t sig = 0;
-    for (int j = 0; j < g.width; j++) sig |= q & (3ull << (2 * g.pos[j]));
-    for (int j = 0; j < g.rwidth; j++) sig |= static_cast<uint64_t>((r >> (2 * j)) & 3u) << (2 * g.rpos[j]);
-    return sig;
 }
 
 struct Contribution {
@@ -491,7 +693,6 @@ __device__ __forceinline__ uint64_t warp_incl_sum_u64(uint64_t v, int lane) {
 }
 
 struct ScoreArgs {
-    uint32_t hit_cap;
     IndexView ix;
     const uint64_t* qsig;
     uint4* seg;
@@ -518,7 +719,7 @@ __global__ void __launch_bounds__(256) k_score_warp(ScoreArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint64_t* keys = s_keys[warp];
     const Tables& T = *a.tables;
-    if (a.counters->n_hits > a.hit_cap || a.counters->overflow) return;  // rerun follows
+    if (a.counters->overflow) return;  // rerun follows
     const uint64_t gw = blockIdx.x * 8ull + warp, nw = gridDim.x * 8ull;
     for (uint64_t qi = gw; qi < a.n; qi += nw) {
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
@@ -558,9 +759,9 @@ __global__ void __launch_bounds__(256) k_score_warp(ScoreArgs a) {
             uint32_t id = 0;
             if (t < L) {
                 const uint4 r = seg[keys[t] & 0xFF];
-                const SliceGeom& g = s_geom[r.y];
                 id = r.w;
-                c = contribution(T, a.P, q, site_signature(q, g, r.z), a.ix.occ[id]);
+                const uint4 sr = a.ix.srec[id];  // signature and occurrences in one read
+                c = contribution(T, a.P, q, (static_cast<uint64_t>(sr.y) << 32) | sr.x, sr.z);
             }
             const double im = warp_incl_sum(c.mit, lane) + run_mit;
             const double ic = warp_incl_sum(c.cfd, lane) + run_cfd;
@@ -580,9 +781,15 @@ __global__ void __launch_bounds__(256) k_score_warp(ScoreArgs a) {
     }
 }
 
-// Block per guide with more than kWarpHits hits: bitonic sort of the segment in global memory
-// (in place), then the same ordered accumulation with block-wide prefix sums.
+// Block per guide with more than kWarpHits hits. Up to kBlockHits hits are sorted in shared
+// memory (keys with the hit index in the low bits); larger segments are sorted in place in
+// global memory. Both use the same one-direction bitonic network as the warp path, then the
+// ordered accumulation runs with block-wide prefix sums.
+constexpr int kBlockHits = 8192;
+constexpr int kBlockIdxBits = 13;
+
 __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
+    extern __shared__ __align__(16) uint64_t s_bkeys[];  // kBlockHits keys
     __shared__ SliceGeom s_geom[kMaxSlices];
     __shared__ double s_wm[8], s_wc[8];
     __shared__ uint64_t s_wn[8];
@@ -591,7 +798,7 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const Tables& T = *a.tables;
-    if (a.counters->n_hits > a.hit_cap || a.counters->overflow) return;  // rerun follows
+    if (a.counters->overflow) return;  // rerun follows
     const uint32_t n_big = a.counters->n_big;
     for (uint32_t b = blockIdx.x; b < n_big; b += gridDim.x) {
         const uint64_t qi = a.big[b];
@@ -600,11 +807,25 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
         const uint64_t q = a.qsig[qi];
         uint32_t P2 = 1;
         while (P2 < L) P2 <<= 1;
+        const bool in_smem = L <= static_cast<uint32_t>(kBlockHits);
+        if (in_smem) {
+            for (uint32_t i = threadIdx.x; i < P2; i += blockDim.x)
+                s_bkeys[i] = i < L ? (order_key(seg[i]) << kBlockIdxBits) | i : ~0ull;
+            __syncthreads();
+        }
         for (uint32_t k = 2; k <= P2; k <<= 1) {
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
                 for (uint32_t i = threadIdx.x; i < P2; i += blockDim.x) {
+                    // first stage of each merge compares mirrored pairs, later stages i / i+j
                     const uint32_t partner = (j == (k >> 1)) ? (i ^ (k - 1)) : (i ^ j);
-                    if (partner > i && partner < L) {
+                    if (partner <= i) continue;
+                    if (in_smem) {
+                        const uint64_t x = s_bkeys[i], y = s_bkeys[partner];
+                        if (x > y) {
+                            s_bkeys[i] = y;
+                            s_bkeys[partner] = x;
+                        }
+                    } else if (partner < L) {
                         const uint4 x = seg[i], y = seg[partner];
                         if (order_key(x) > order_key(y)) {
                             seg[i] = y;
@@ -623,9 +844,10 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             Contribution c{0.0, 0.0, 0};
             uint32_t id = 0;
             if (t < L) {
-                const uint4 r = seg[t];
+                const uint4 r = in_smem ? seg[s_bkeys[t] & ((1u << kBlockIdxBits) - 1)] : seg[t];
                 id = r.w;
-                c = contribution(T, a.P, q, site_signature(q, s_geom[r.y], r.z), a.ix.occ[id]);
+                const uint4 sr = a.ix.srec[id];
+                c = contribution(T, a.P, q, (static_cast<uint64_t>(sr.y) << 32) | sr.x, sr.z);
             }
             double im = warp_incl_sum(c.mit, lane), ic = warp_incl_sum(c.cfd, lane);
             uint64_t in = warp_incl_sum_u64(c.occ, lane);
@@ -685,6 +907,15 @@ __global__ void k_copy_distinct(const Counters* c, uint64_t* out) { *out = c->di
 
 // ---------------------------------------------------------------------------------------------
 // host orchestration
+const void* scan_kernel(int rw) {
+    switch (rw) {
+        case 12: return reinterpret_cast<const void*>(&k_scan<12>);
+        case 10: return reinterpret_cast<const void*>(&k_scan<10>);
+        case 16: return reinterpret_cast<const void*>(&k_scan<16>);
+        default: return reinterpret_cast<const void*>(&k_scan<0>);
+    }
+}
+
 int sm_count(int device) {
     int v = 0;
     cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
@@ -715,7 +946,20 @@ Workspace& workspace(issl_index* ix) {
         ISSL_CUDA(cudaStreamCreateWithFlags(&ws->own_stream, cudaStreamNonBlocking));
         for (auto& e : ws->ev) ISSL_CUDA(cudaEventCreate(&e));
         int per_sm = 0;
-        ISSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan, kScanWarps * 32, 0));
+        uint32_t max_wpb = 4;
+        for (auto& g : ix->geom) max_wpb = std::max<uint32_t>(max_wpb, g.wpb);
+        ws->scan_layout = warp_layout(max_wpb);
+        ws->scan_smem = static_cast<int>(kScanWarps * ws->scan_layout.bytes);
+        // one residual width for every slice (the usual case) selects a specialised scan
+        ws->scan_rw = ix->geom.empty() ? 0 : ix->geom[0].rwidth;
+        for (auto& g : ix->geom)
+            if (g.rwidth != ws->scan_rw) ws->scan_rw = 0;
+        if (ws->scan_rw != 12 && ws->scan_rw != 10 && ws->scan_rw != 16) ws->scan_rw = 0;
+        const void* kfn = scan_kernel(ws->scan_rw);
+        ISSL_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, ws->scan_smem));
+        ISSL_CUDA(cudaFuncSetAttribute(k_score_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(kBlockHits * sizeof(uint64_t))));
+        ISSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kScanWarps * 32, ws->scan_smem));
         ws->scan_blocks = sm_count(ix->device) * std::max(per_sm, 1);
         ws->counters.reserve(1);
         ws->scan64.reserve(kScanBlocks + 4);
@@ -738,8 +982,7 @@ void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, cudaStream_t st) {
         const size_t cap = std::max<size_t>(n, 1024);
         ws.qsig.reserve(cap);
         ws.probe_gb.reserve(cap * S);
-        ws.probe_q.reserve(cap * S);
-        ws.probe_rq.reserve(cap * S);
+        ws.probe_qr.reserve(cap * S + 2);
         ws.qhits.reserve(cap + 1);
         ws.qhoff.reserve(cap + 1);
         ws.big.reserve(cap);
@@ -762,11 +1005,13 @@ void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, cudaStream_t st) {
         ws.units.reserve(want_units);
         ws.unit_cap = want_units;
     }
-    const size_t want_hits = std::max<size_t>(ws.hit_cap, n * 64 + 65536);
-    if (ws.hit_cap < want_hits) {
-        ws.hits.reserve(want_hits);
-        ws.seg.reserve(want_hits);
-        ws.hit_cap = want_hits;
+    // candidates: a first guess plus one slab of slack per scan warp; grown on demand
+    const size_t want_cands = std::max<size_t>(
+        ws.cand_cap, n * 64 + 65536 + static_cast<size_t>(ws.scan_blocks) * kScanWarps * kCandSlab);
+    if (ws.cand_cap < want_cands) {
+        ws.cands.reserve(want_cands);
+        ws.seg.reserve(want_cands);
+        ws.cand_cap = want_cands;
     }
 }
 
@@ -803,37 +1048,41 @@ void enqueue_pipeline(issl_index* ix, Workspace& ws, const uint64_t* d_qsig, uin
     const uint64_t* off = ix->offsets.p;
     ISSL_CUDA(cudaEventRecord(ws.ev[0], st));
     k_probe_count<<<grid_for(n * S, 256, sms * 16), 256, 0, st>>>(v, d_qsig, n, ws.probe_gb.p, ws.bucket_cnt.p, off);
-    device_scan<uint64_t, OpSum>(BucketLoad{ws.bucket_cnt.p, off},
+    device_scan<uint64_t, OpSum>(BucketLoad{ws.bucket_cnt.p, off, ix->n_sites},
                                  BucketStore{ws.bucket_cnt.p, off, ws.bucket_qstart.p, ws.units.p, ws.unit_cap,
                                              ix->n_sites},
                                  nullptr, G, ws.scan64.p, &ws.counters.p->bucket_total, st);
     k_units_finalize<<<1, 1, 0, st>>>(ws.counters.p, ws.unit_cap);
-    k_bucket_stats<<<sms * 4, 256, 0, st>>>(ws.bucket_cnt.p, off, G, ws.counters.p);
+    k_bucket_stats<<<sms * 4, 256, 0, st>>>(ws.bucket_cnt.p, off, G, ix->d_geom.p, ix->n_sites, ws.counters.p);
     k_probe_scatter<<<grid_for(n * S, 256, sms * 16), 256, 0, st>>>(v, d_qsig, n, ws.probe_gb.p, ws.bucket_cnt.p,
-                                                                     ws.bucket_qstart.p, ws.probe_q.p, ws.probe_rq.p);
+                                                                     ws.bucket_qstart.p, ws.probe_qr.p);
     ScanArgs sa;
-    sa.resid = ix->resid.p;
+    sa.rbits = ix->rbits.p;
     sa.geom = ix->d_geom.p;
     sa.units = ws.units.p;
-    sa.probe_q = ws.probe_q.p;
-    sa.probe_rq = ws.probe_rq.p;
+    sa.probe_qr = ws.probe_qr.p;
     sa.counters = ws.counters.p;
-    sa.hits = ws.hits.p;
-    sa.qhits = ws.qhits.p;
-    sa.n_sites = ix->n_sites;
-    sa.hit_cap = static_cast<uint32_t>(std::min<size_t>(ws.hit_cap, 0xFFFFFFFFull));
+    sa.cands = ws.cands.p;
     sa.n_slices = static_cast<uint32_t>(S);
+    sa.cand_cap = static_cast<uint32_t>(std::min<size_t>(ws.cand_cap, 0xFFFFFFFFull));
     sa.max_dist = P.max_dist;
+    sa.L = ws.scan_layout;
     ISSL_CUDA(cudaEventRecord(ws.ev[1], st));
-    k_scan<<<ws.scan_blocks, kScanWarps * 32, 0, st>>>(sa);
+    switch (ws.scan_rw) {
+        case 12: k_scan<12><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
+        case 10: k_scan<10><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
+        case 16: k_scan<16><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
+        default: k_scan<0><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
+    }
     ISSL_CUDA(cudaEventRecord(ws.ev[2], st));
+    k_cands_finalize<<<1, 1, 0, st>>>(ws.counters.p, sa.cand_cap);
+    k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, v, ws.qhits.p);
     device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, nullptr, n, ws.scan32.p,
                                  ws.qhoff.p + n, st);
-    k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.hits.p, ws.counters.p, sa.hit_cap, ws.qhits.p, ws.qhoff.p, ix->ids.p,
+    k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, ws.qhits.p, ws.qhoff.p, ix->ids.p,
                                            ix->n_sites, ws.seg.p);
     if (P.want_distinct) ISSL_CUDA(cudaMemsetAsync(ws.bitmap.p, 0, (ix->n_sites / 32 + 1) * 4, st));
     ScoreArgs a;
-    a.hit_cap = sa.hit_cap;
     a.ix = v;
     a.qsig = d_qsig;
     a.seg = ws.seg.p;
@@ -849,21 +1098,27 @@ void enqueue_pipeline(issl_index* ix, Workspace& ws, const uint64_t* d_qsig, uin
     a.out_code = d_code;
     a.out_count = d_count;
     k_score_warp<<<grid_for(n, 8, sms * 8), 256, 0, st>>>(a);
-    k_score_block<<<sms * 2, 256, 0, st>>>(a);
+    k_score_block<<<sms * 2, 256, kBlockHits * sizeof(uint64_t), st>>>(a);
     if (P.want_distinct) k_popcount<<<sms * 4, 256, 0, st>>>(ws.bitmap.p, ix->n_sites / 32 + 1, ws.counters.p);
     ISSL_CUDA(cudaEventRecord(ws.ev[3], st));
     ISSL_CUDA(cudaGetLastError());
-    // probe_count, 3 bucket-scan, units_finalize, bucket_stats, probe_scatter, scan, 3 hit-offset
-    // scan, hit_scatter, score_warp, score_block (+ popcount for distinct counts)
-    ws.launches += 14 + (P.want_distinct ? 1 : 0);
+    // probe_count, 3 bucket-scan, units_finalize, bucket_stats, probe_scatter, scan,
+    // cands_finalize, cand_own, 3 hit-offset scan, hit_scatter, score_warp, score_block
+    // (+ popcount for distinct counts)
+    ws.launches += 16 + (P.want_distinct ? 1 : 0);
 }
 
 // Reads the counters after a pipeline run; returns false (and grows capacities) on overflow.
-bool check_and_grow(issl_index* ix, Workspace& ws, cudaStream_t st) {
+bool check_and_grow(issl_index* ix, Workspace& ws, uint64_t n, cudaStream_t st) {
     Counters c;
     ISSL_CUDA(cudaMemcpyAsync(&c, ws.counters.p, sizeof c, cudaMemcpyDeviceToHost, st));
+    ISSL_CUDA(cudaMemcpyAsync(&c.hit_total, ws.qhoff.p + n, 4, cudaMemcpyDeviceToHost, st));
     ISSL_CUDA(cudaStreamSynchronize(st));
     ws.last = c;
+    if (c.overflow & 4u) {
+        ws.zero_state_ok = false;
+        throw Error(ISSL_ERR_TIMEOUT, "scan: an asynchronous copy did not complete within the wait limit");
+    }
     const uint64_t units = c.bucket_total >> 32;
     bool ok = true;
     if (units > ws.unit_cap) {
@@ -871,12 +1126,13 @@ bool check_and_grow(issl_index* ix, Workspace& ws, cudaStream_t st) {
         ws.unit_cap = units + units / 8 + 1024;
         ok = false;
     }
-    if (c.n_hits > ws.hit_cap) {
-        const size_t cap = static_cast<size_t>(c.n_hits) + c.n_hits / 4 + 65536;
-        ISSL_REQUIRE(cap < 0xFFFFFFFFull, ISSL_ERR_UNSUPPORTED, "more than 2^32 hits in one call; split the guides");
-        ws.hits.reserve(cap);
+    if (c.n_cand > ws.cand_cap || (c.overflow & 2u)) {
+        const size_t cap = static_cast<size_t>(c.n_cand) + c.n_cand / 4 + 65536;
+        ISSL_REQUIRE(cap < 0xFFFFFFFFull, ISSL_ERR_UNSUPPORTED,
+                     "more than 2^32 candidate sites in one call; split the guides");
+        ws.cands.reserve(cap);
         ws.seg.reserve(cap);
-        ws.hit_cap = cap;
+        ws.cand_cap = cap;
         ok = false;
     }
     if (!ok) ws.zero_state_ok = false;  // counters of the aborted run are not drained
@@ -892,12 +1148,12 @@ void record_stats(issl_index* ix, Workspace& ws, uint64_t n) {
     s.total_ms = total;
     s.probes = static_cast<uint64_t>(ws.last.bucket_total & 0xFFFFFFFFull);
     s.units = ws.last.bucket_total >> 32;
-    s.hits = ws.last.n_hits;
+    s.hits = ws.last.hit_total;
     s.buckets_scanned = ws.last.buckets;
     s.entries_scanned = ws.last.entries;
-    // bytes the scan must move: 4 per residual streamed, 16 per unit descriptor, 8 per guide of
-    // a unit (slot + residual), 16 per hit written
-    s.scan_bytes = 4 * s.entries_scanned + 16 * s.units + 8 * s.probes + 16 * s.hits;
+    // bytes the scan must move: the bit-sliced blocks it copies, 16 per unit descriptor, 8 per
+    // guide of a unit (index + residual), 16 per candidate slot written
+    s.scan_bytes = ws.last.rbytes + 16 * s.units + 8 * s.probes + 16 * static_cast<uint64_t>(ws.last.n_cand);
     s.launches = ws.launches;
     ws.launches = 0;
     (void)n;
@@ -918,7 +1174,7 @@ void run_scoring(issl_index* ix, const uint64_t* d_qsig_in, uint64_t n, const Sc
         if (!sync_and_check) {
             // device-buffer path: one check per call keeps the workspace honest
         }
-        if (check_and_grow(ix, ws, st)) {
+        if (check_and_grow(ix, ws, n, st)) {
             record_stats(ix, ws, n);
             return;
         }
@@ -946,8 +1202,8 @@ int issl_score_device(issl_index* ix, const uint64_t* d_sigs, size_t n, int meth
             if (d_distinct) ISSL_CUDA(cudaMemsetAsync(d_distinct, 0, 8, st));
             return;
         }
-        ISSL_REQUIRE(n < (1ull << 31) && n * ix->n_slices < 0xFFFFFFFFull, ISSL_ERR_ARG,
-                     "too many guides in one call");
+        ISSL_REQUIRE(n < (1ull << issl::kGuideBits) && n * ix->n_slices < 0xFFFFFFFFull, ISSL_ERR_ARG,
+                     "too many guides in one call (at most 2^26 and 2^32 guide-slice pairs)");
         issl::run_scoring(ix, d_sigs, n, P, d_mit, d_cfd, d_code, d_count, d_distinct, st, true);
     });
 }
@@ -967,8 +1223,8 @@ static int score_host_common(issl_index* ix, const char* seqs, size_t stride, co
             if (distinct) *distinct = 0;
             return;
         }
-        ISSL_REQUIRE(n < (1ull << 31) && n * ix->n_slices < 0xFFFFFFFFull, ISSL_ERR_ARG,
-                     "too many guides in one call");
+        ISSL_REQUIRE(n < (1ull << issl::kGuideBits) && n * ix->n_slices < 0xFFFFFFFFull, ISSL_ERR_ARG,
+                     "too many guides in one call (at most 2^26 and 2^32 guide-slice pairs)");
         issl::ensure_capacity(ix, ws, n, st);
         if (seqs) {
             const size_t bytes = (n - 1) * stride + issl::kSeqLen;

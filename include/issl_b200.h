@@ -99,7 +99,8 @@ int issl_save(const issl_index* index, const char* path);
  *   code[i]:      ISSL_CODE_ACCEPTED / ISSL_CODE_REJECTED by the method's rule
  *   count[i]:     sum of occurrences of the scored sites (ISSLScoreOfftargets.cpp:371)
  * distinct (optional): number of distinct sites scored over all guides (:375-377).
- * Any output pointer except code may be NULL. max_dist: 0..4 (the reference fixes 4). */
+ * Any output pointer except code may be NULL. max_dist: 0..4 (the reference fixes 4).
+ * One call takes at most 2^26 guides (and fewer than 2^32 guide-slice pairs). */
 int issl_score(issl_index* index, const char* seqs, size_t stride, size_t n, int method,
                double threshold, int max_dist, double* mit_score, double* cfd_score, char* code,
                uint64_t* count, uint64_t* distinct);

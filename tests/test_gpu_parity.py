@@ -262,3 +262,19 @@ def test_corrupt_indexes_rejected(native, oracle_arrays, tmp_path):
     with pytest.raises(native.IsslError) as e:
         native.Index.from_arrays(sigs, masks, sizes, lists).score(["A" * 20], "and", 75.0, max_dist=5)
     assert e.value.code == -1
+
+
+def test_mixed_slice_widths_use_generic_scan(native, oracle):
+    """Slices of different widths (the format allows it) go through the mixed-width scan."""
+    import synth
+    sites, occ, queries = synth.make_case(21, 30000, 200, repeat_frac=0.1, n_seeds=20)
+    masks = synth.masks_from_strings([
+        "11111100000000000000", "00000011111110000000", "00000000000001111111",
+        "10101010101010101010", "01010101010101010101", "11110000111100001111",
+    ])
+    oix = oracle.Index.build(sites, occ, masks)
+    with native.Index.from_arrays(*oix.arrays()) as ix:
+        for meth, t in [("mitAndCfd", 75.0), ("avgMitCfd", 95.0), ("cfd", 99.0)]:
+            tm, tc, cnt, dist = oix.score(queries, METHODS[meth], t)
+            ms, cs, codes = oracle.finalise(METHODS[meth], t, tm, tc)
+            assert_matches(ix.score(queries, meth, t), ms, cs, codes, cnt, dist, tag=f"mixed {meth}")
