@@ -69,6 +69,7 @@ SIGNATURES = [
     ("issl_score_sigs", C.c_int, [vp, u64p, C.c_size_t, C.c_int, C.c_double, C.c_int, f64p, f64p, C.c_char_p,
                                   u64p, u64p]),
     ("issl_score_device", C.c_int, [vp, vp, C.c_size_t, C.c_int, C.c_double, C.c_int, vp, vp, vp, vp, vp, vp]),
+    ("issl_score_device_static", C.c_int, [vp, vp, C.c_size_t, C.c_int, C.c_double, C.c_int, vp, vp, vp, vp, vp]),
     ("issl_last_stats", C.c_int, [vp, P(ScoreStats)]),
     ("issl_synth", C.c_int, [P(SynthSpecC), C.c_int, P(vp), u64p]),
     ("issl_tables", C.c_int, [u64p, f64p, f64p, f64p]),

@@ -24,6 +24,8 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "async_copy.cuh"
@@ -1268,3 +1270,287 @@ int issl_last_stats(const issl_index* ix, issl_score_stats* out) {
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Allocation-free scoring.
+//
+// Some callers cannot allocate device memory when they score: code that runs while a stream is
+// being captured into a CUDA graph, hosts that hand all device memory to their own pool
+// allocator (a framework's caching allocator, a fixed arena on a shared GPU) and forbid stray
+// cudaMalloc calls, and latency-bound services that allow no allocation after start-up. The
+// regular entry points grow a per-index workspace on demand; issl_score_device_static instead
+// runs one kernel whose only scratch is the file-scope array below, fixed at library load.
+//
+// One block scores one guide at a time (grid-stride over the guides): for every slice it walks
+// the guide's bucket block by block with the bit-sliced comparison, applies the ownership rule
+// to each candidate, stores the owned hits of the guide in its block's slice of g_static_hits,
+// sorts them in shared memory in the order the reference visits them, and accumulates MIT and
+// CFD with the reference's early exit.
+// =============================================================================================
+namespace issl {
+namespace {
+
+constexpr int kStaticBlocks = 148;                       // scoring blocks (one per B200 SM)
+constexpr int kStaticThreads = 256;
+constexpr uint32_t kStaticHits = ISSL_STATIC_MAX_HITS;   // owned hits per guide
+constexpr uint32_t kStaticIdxBits = 12;                  // log2(kStaticHits)
+static_assert((1u << kStaticIdxBits) == kStaticHits, "hit index bits");
+
+// 148 blocks x 4096 hits x 16 bytes = 9.7 MB, held by every GPU that loads the library
+static __device__ __align__(256) uint4 g_static_hits[kStaticBlocks * kStaticHits];
+// [0]: a guide had more than kStaticHits owned hits (cleared by every call)
+static __device__ __align__(256) uint32_t g_static_status[4];
+static __device__ __align__(256) Tables g_static_tables;
+
+struct StaticArgs {
+    IndexView ix;
+    const uint64_t* qsig;
+    uint64_t n;
+    ScoreParams P;
+    const Tables* tables;
+    uint4* hits;
+    uint32_t* status;
+    double* out_mit;
+    double* out_cfd;
+    char* out_code;
+    uint64_t* out_count;
+};
+
+// Bit-sliced comparison of one block (32 list positions) of slice s with the guide; owned hits
+// are appended to the block's hit area.
+template <int RW>
+__device__ __forceinline__ void static_block(const StaticArgs& a, const SliceGeom* geom, uint32_t s, uint64_t b,
+                                             uint32_t e0, uint32_t e1, const uint32_t* qm, uint4* hits,
+                                             uint32_t* cnt) {
+    constexpr int NW = 2 * RW;
+    const SliceGeom& g = geom[s];
+    const uint32_t* blk = a.ix.rbits + g.wbase + b * g.wpb;
+    uint32_t mm[RW];
+#pragma unroll
+    for (int p = 0; p < RW; p++) mm[p] = (blk[2 * p] ^ qm[2 * p]) | (blk[2 * p + 1] ^ qm[2 * p + 1]);
+    const int lo = max(static_cast<int>(e0) - static_cast<int>(32 * b), 0);
+    const int hi = min(static_cast<int>(e1) - static_cast<int>(32 * b), 32);
+    const uint32_t valid = (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
+    uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), a.P.max_dist) & valid;
+    (void)NW;
+    while (cbits) {
+        const int e = __ffs(cbits) - 1;
+        cbits &= cbits - 1;
+        uint32_t rm = 0, mism20 = 0;
+#pragma unroll
+        for (int p = 0; p < RW; p++) rm |= ((mm[p] >> e) & 1u) << p;
+        for (uint32_t t = rm; t; t &= t - 1) mism20 |= 1u << g.rpos[__ffs(t) - 1];
+        bool own = true;
+        for (uint32_t t = 0; t < s; t++)
+            if ((mism20 & geom[t].pmask) == 0) {
+                own = false;  // an earlier slice reaches this site
+                break;
+            }
+        if (!own) continue;
+        const uint32_t pos = static_cast<uint32_t>(32 * b) + e;
+        const uint32_t slot = atomicAdd(cnt, 1u);
+        if (slot < kStaticHits)
+            hits[slot] = make_uint4(pos, s, rm, a.ix.ids[static_cast<uint64_t>(s) * a.ix.n_sites + pos]);
+    }
+}
+
+__global__ void __launch_bounds__(kStaticThreads) k_score_static(StaticArgs a) {
+    __shared__ uint64_t s_keys[kStaticHits];
+    __shared__ SliceGeom s_geom[kMaxSlices];
+    __shared__ uint32_t s_qm[32];
+    __shared__ uint32_t s_cnt;
+    __shared__ double s_wm[kStaticThreads / 32], s_wc[kStaticThreads / 32];
+    __shared__ uint64_t s_wn[kStaticThreads / 32];
+    __shared__ int s_first;
+    for (int i = threadIdx.x; i < static_cast<int>(a.ix.n_slices); i += blockDim.x) s_geom[i] = a.ix.geom[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const Tables& T = *a.tables;
+    uint4* hits = a.hits + static_cast<size_t>(blockIdx.x) * kStaticHits;
+    for (uint64_t qi = blockIdx.x; qi < a.n; qi += gridDim.x) {
+        const uint64_t q = a.qsig[qi];
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        for (uint32_t s = 0; s < a.ix.n_slices; s++) {
+            const SliceGeom& g = s_geom[s];
+            const uint32_t gb = g.bbase + slice_key(q, g);
+            const uint64_t base = static_cast<uint64_t>(s) * a.ix.n_sites;
+            const uint32_t e0 = static_cast<uint32_t>(a.ix.offsets[gb] - base);
+            const uint32_t e1 = static_cast<uint32_t>(a.ix.offsets[gb + 1] - base);
+            const uint32_t rq = slice_residual(q, g);
+            if (threadIdx.x < 2u * g.rwidth) s_qm[threadIdx.x] = 0u - ((rq >> threadIdx.x) & 1u);
+            __syncthreads();
+            if (e1 > e0) {
+                for (uint64_t b = e0 / 32 + threadIdx.x; b <= (e1 - 1) / 32; b += blockDim.x) {
+                    switch (g.rwidth) {
+                        case 12: static_block<12>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                        case 10: static_block<10>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                        case 16: static_block<16>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                        case 15: static_block<15>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                        case 14: static_block<14>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                        case 13: static_block<13>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                        case 11: static_block<11>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                        case 9: static_block<9>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                        case 8: static_block<8>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                        default: static_block<7>(a, s_geom, s, b, e0, e1, s_qm, hits, &s_cnt); break;
+                    }
+                }
+            }
+            __syncthreads();  // s_qm is rewritten for the next slice
+        }
+        const uint32_t L = s_cnt;
+        if (L > kStaticHits) {
+            if (threadIdx.x == 0) atomicOr(&a.status[0], 1u);
+            __syncthreads();
+            continue;
+        }
+        // the reference's visiting order: slice, then list position
+        uint32_t P2 = 1;
+        while (P2 < L) P2 <<= 1;
+        for (uint32_t i = threadIdx.x; i < P2; i += blockDim.x)
+            s_keys[i] = i < L ? (((static_cast<uint64_t>(hits[i].y) << 32) | hits[i].x) << kStaticIdxBits) | i : ~0ull;
+        __syncthreads();
+        for (uint32_t k = 2; k <= P2; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = threadIdx.x; i < P2; i += blockDim.x) {
+                    const uint32_t partner = (j == (k >> 1)) ? (i ^ (k - 1)) : (i ^ j);
+                    if (partner > i) {
+                        const uint64_t x = s_keys[i], y = s_keys[partner];
+                        if (x > y) {
+                            s_keys[i] = y;
+                            s_keys[partner] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        double run_mit = 0.0, run_cfd = 0.0;
+        uint64_t run_cnt = 0;
+        bool stopped = false;
+        for (uint32_t c0 = 0; c0 < L && !stopped; c0 += blockDim.x) {
+            const uint32_t t = c0 + threadIdx.x;
+            Contribution c{0.0, 0.0, 0};
+            if (t < L) {
+                const uint4 r = hits[s_keys[t] & (kStaticHits - 1)];
+                const uint4 sr = a.ix.srec[r.w];
+                c = contribution(T, a.P, q, (static_cast<uint64_t>(sr.y) << 32) | sr.x, sr.z);
+            }
+            double im = warp_incl_sum(c.mit, lane), ic = warp_incl_sum(c.cfd, lane);
+            uint64_t in = warp_incl_sum_u64(c.occ, lane);
+            if (lane == 31) {
+                s_wm[warp] = im;
+                s_wc[warp] = ic;
+                s_wn[warp] = in;
+            }
+            if (threadIdx.x == 0) s_first = 0x7fffffff;
+            __syncthreads();
+            double pm = run_mit, pc = run_cfd;
+            uint64_t pn = run_cnt;
+            for (int w = 0; w < warp; w++) {
+                pm += s_wm[w];
+                pc += s_wc[w];
+                pn += s_wn[w];
+            }
+            im += pm;
+            ic += pc;
+            in += pn;
+            if (t < L && exit_test(a.P, im, ic)) atomicMin(&s_first, static_cast<int>(threadIdx.x));
+            __syncthreads();
+            const int first = s_first;
+            const uint32_t in_chunk = L - c0 < blockDim.x ? L - c0 : blockDim.x;
+            const int last = first != 0x7fffffff ? first : static_cast<int>(in_chunk) - 1;
+            __syncthreads();
+            if (static_cast<int>(threadIdx.x) == last) {
+                s_wm[0] = im;
+                s_wc[0] = ic;
+                s_wn[0] = in;
+            }
+            __syncthreads();
+            run_mit = s_wm[0];
+            run_cfd = s_wc[0];
+            run_cnt = s_wn[0];
+            stopped = first != 0x7fffffff;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            finalise(a.P, run_mit, run_cfd, run_cnt, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+        __syncthreads();
+    }
+}
+
+// Device addresses of the static scratch, looked up once per device with that device current.
+struct StaticScratch {
+    bool ready = false;
+    uint4* hits = nullptr;
+    uint32_t* status = nullptr;
+    Tables* tables = nullptr;
+};
+std::mutex g_static_mu;
+StaticScratch g_static[64];
+
+StaticScratch& static_scratch(int device) {
+    ISSL_REQUIRE(device >= 0 && device < 64, ISSL_ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    StaticScratch& sc = g_static[device];
+    if (!sc.ready) {
+        // the host-side names of the arrays are stand-ins, not device addresses
+        ISSL_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.hits), g_static_hits));
+        ISSL_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.status), g_static_status));
+        ISSL_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.tables), g_static_tables));
+        Tables h;
+        const auto& mit = mit_rank_table();
+        std::memcpy(h.mit, mit.data(), sizeof h.mit);
+        std::memcpy(h.cfd_pos, cfd_pos_table(), sizeof h.cfd_pos);
+        std::memcpy(h.cfd_pam, cfd_pam_table(), sizeof h.cfd_pam);
+        for (int p = 0; p < 20; p++)
+            for (int i = 0; i < 5; i++) {
+                uint64_t r = (i <= p) ? 1 : 0;
+                for (int t = 1; t <= i && i <= p; t++) r = r * (p - i + t) / t;
+                h.binom[p][i] = static_cast<uint32_t>(r);
+            }
+        ISSL_CUDA(cudaMemcpy(sc.tables, &h, sizeof h, cudaMemcpyHostToDevice));
+        sc.ready = true;
+    }
+    return sc;
+}
+
+}  // namespace
+}  // namespace issl
+
+extern "C" int issl_score_device_static(issl_index* ix, const uint64_t* d_sigs, size_t n, int method,
+                                        double threshold, int max_dist, double* d_mit, double* d_cfd, char* d_code,
+                                        uint64_t* d_count, void* stream) {
+    return issl::guarded([&] {
+        ISSL_REQUIRE(ix && (d_sigs || n == 0) && d_code, ISSL_ERR_ARG, "issl_score_device_static: null argument");
+        ISSL_REQUIRE(n <= ISSL_STATIC_MAX_GUIDES, ISSL_ERR_ARG,
+                     "issl_score_device_static: at most " + std::to_string(ISSL_STATIC_MAX_GUIDES) +
+                         " guides per call");
+        const issl::ScoreParams P = issl::make_params(method, threshold, max_dist, false);
+        ISSL_CUDA(cudaSetDevice(ix->device));
+        issl::StaticScratch& sc = issl::static_scratch(ix->device);
+        if (n == 0) return;
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        ISSL_CUDA(cudaMemsetAsync(sc.status, 0, sizeof(uint32_t), st));
+        issl::StaticArgs a;
+        a.ix = ix->view();
+        a.qsig = d_sigs;
+        a.n = n;
+        a.P = P;
+        a.tables = sc.tables;
+        a.hits = sc.hits;
+        a.status = sc.status;
+        a.out_mit = d_mit;
+        a.out_cfd = d_cfd;
+        a.out_code = d_code;
+        a.out_count = d_count;
+        issl::k_score_static<<<issl::kStaticBlocks, issl::kStaticThreads, 0, st>>>(a);
+        ISSL_CUDA(cudaGetLastError());
+        uint32_t status = 0;
+        ISSL_CUDA(cudaMemcpyAsync(&status, sc.status, sizeof status, cudaMemcpyDeviceToHost, st));
+        ISSL_CUDA(cudaStreamSynchronize(st));
+        ISSL_REQUIRE(status == 0, ISSL_ERR_UNSUPPORTED,
+                     "issl_score_device_static: a guide has more than " + std::to_string(ISSL_STATIC_MAX_HITS) +
+                         " off-target hits; score it with issl_score_device");
+    });
+}

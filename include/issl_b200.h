@@ -117,6 +117,29 @@ int issl_score_device(issl_index* index, const uint64_t* d_sigs, size_t n, int m
                       double threshold, int max_dist, double* d_mit_score, double* d_cfd_score,
                       char* d_code, uint64_t* d_count, uint64_t* d_distinct, void* stream);
 
+/* Allocation-free scoring. No counterpart in the reference, which scores on the CPU.
+ *
+ * For callers that cannot allocate device memory while they score: code running during CUDA
+ * graph capture, hosts whose device memory belongs to their own pool allocator, services that
+ * allow no allocation after start-up. The regular entry points grow a per-index workspace on
+ * demand; this one allocates nothing (no cudaMalloc, no cudaFree, no allocating library call).
+ * Its only scratch is a fixed 9.7 MB array inside the library, which every GPU that loads the
+ * library holds until the process exits.
+ *
+ * Same arguments and results as issl_score_device (minus the distinct count), buffers in device
+ * memory of the index's device, enqueued on `stream` (NULL = the default stream); the call waits
+ * for the kernel to finish. Limits: at most ISSL_STATIC_MAX_GUIDES guides per call (larger n is
+ * rejected with ISSL_ERR_ARG) and at most ISSL_STATIC_MAX_HITS owned off-target hits per guide
+ * (a guide beyond that makes the call fail with ISSL_ERR_UNSUPPORTED; its outputs are not set).
+ * The first call on a device looks up the scratch address and uploads the penalty tables; make
+ * that first call before any stream capture. Every call shares the one scratch array, so calls
+ * that overlap on the GPU (concurrent streams or threads) race and must be serialised. */
+#define ISSL_STATIC_MAX_GUIDES 1048576
+#define ISSL_STATIC_MAX_HITS 4096
+int issl_score_device_static(issl_index* index, const uint64_t* d_sigs, size_t n, int method,
+                             double threshold, int max_dist, double* d_mit_score, double* d_cfd_score,
+                             char* d_code, uint64_t* d_count, void* stream);
+
 /* Kernel timing of the last issl_score* call on this index (device milliseconds of the scan
  * kernel and of the whole pipeline, taken with CUDA events on its stream) and its work
  * counters: probes, distinct buckets scanned, entries streamed, scan units, owned hits, the
