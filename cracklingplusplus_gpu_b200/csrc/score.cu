@@ -38,7 +38,6 @@ namespace issl {
 
 constexpr int kChunk = 1024;       // list positions per scan unit: 32 bit-sliced blocks of 32
 constexpr int kGroup = 32;         // guides per scan unit
-constexpr int kWarpHits = 256;     // guides with more hits are scored by a whole block
 constexpr int kScanWarps = 4;      // warps per scan block
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 
@@ -56,7 +55,8 @@ struct Counters {
     uint32_t n_units;       // min(units, capacity)
     uint32_t n_cand;        // hit slots reserved by the scan (may exceed capacity -> overflow)
     uint32_t hit_total;     // owned hits: sum of per-guide hits (scan total)
-    uint32_t n_big;         // guides deferred to the block scorer
+    uint32_t n_big;         // exiting guides with more than kWarpSort hits (block scorer)
+    uint32_t n_exit;        // exiting guides with at most kWarpSort hits (warp scorer)
     uint32_t overflow;      // 1: units, 2: hits, 4: a bounded wait in the scan gave up
     uint32_t pad;
     uint64_t distinct;
@@ -137,7 +137,8 @@ struct issl::Workspace {
     DevBuf<uint32_t> bucket_cnt, bucket_qstart;
     DevBuf<UnitDesc> units;
     DevBuf<uint4> cands, seg;  // candidate slots; owned hits grouped per guide
-    DevBuf<uint32_t> qhits, qhoff, big;
+    DevBuf<uint32_t> qhits, qhoff, big, exitq;
+    DevBuf<uint64_t> segsig;  // signature of each grouped hit
     DevBuf<uint32_t> bitmap;
     DevBuf<Counters> counters;
     DevBuf<uint64_t> scan64;
@@ -581,20 +582,26 @@ struct StoreQoff {
     __device__ void operator()(uint64_t i, uint32_t ex, uint32_t) const { p[i] = ex; }
 };
 
+// One thread per owned hit (many independent loads in flight): the site id, then the site record
+// (signature, occurrences), written into the guide's segment so that the scorers read only
+// contiguous data.
 __global__ void k_hit_scatter(const uint4* __restrict__ cands, const Counters* c, uint32_t* __restrict__ qhits,
-                              const uint32_t* __restrict__ qhoff, const uint32_t* __restrict__ ids, uint64_t n_sites,
-                              uint4* __restrict__ seg) {
+                              const uint32_t* __restrict__ qhoff, IndexView ix, uint4* __restrict__ seg,
+                              uint64_t* __restrict__ segsig) {
     if (c->overflow) return;
     const uint32_t n = c->n_cand;
     for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x) {
         const uint4 r = cands[h];
         if (r.x == kDeadCand) continue;
         const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
+        const uint32_t sl = r.x >> kGuideBits;
+        const uint32_t id = ix.ids[static_cast<uint64_t>(sl) * ix.n_sites + r.y];
+        const uint4 sr = ix.srec[id];
         // the decrement leaves qhits all zero for the next call
         const uint32_t slot = qhoff[q] + atomicSub(&qhits[q], 1u) - 1u;
-        // seg record: (list position, slice, residual mismatch mask, site id)
-        const uint32_t sl = r.x >> kGuideBits;
-        seg[slot] = make_uint4(r.y, sl, r.z, ids[static_cast<uint64_t>(sl) * n_sites + r.y]);
+        // seg record: (list position, slice, site id, occurrences) + the site signature
+        seg[slot] = make_uint4(r.y, sl, id, sr.z);
+        segsig[slot] = (static_cast<uint64_t>(sr.y) << 32) | sr.x;
     }
 }
 
@@ -698,10 +705,12 @@ struct ScoreArgs {
     IndexView ix;
     const uint64_t* qsig;
     uint4* seg;
+    uint64_t* segsig;
     const uint32_t* qhoff;
     const Tables* tables;
     Counters* counters;
     uint32_t* big;
+    uint32_t* exitq;
     uint32_t* bitmap;
     uint64_t n;
     ScoreParams P;
@@ -711,93 +720,243 @@ struct ScoreArgs {
     uint64_t* out_count;
 };
 
-// Warp per guide; hits (<= kWarpHits) sorted in shared memory by a bitonic network whose
-// comparators all point the same way, so missing elements past L act as +infinity.
-__global__ void __launch_bounds__(256) k_score_warp(ScoreArgs a) {
-    __shared__ uint64_t s_keys[8][kWarpHits];
-    __shared__ SliceGeom s_geom[kMaxSlices];
-    for (int i = threadIdx.x; i < static_cast<int>(a.ix.n_slices); i += blockDim.x) s_geom[i] = a.ix.geom[i];
-    __syncthreads();
+// Exact sums. Every contribution (MIT value x occurrences, CFD product x occurrences) lies in
+// [6e-6, 2^33) and has no bit below 2^-84, so it converts exactly to a 128-bit fixed point
+// value hi * 2^-20 + lo * 2^-84. Integer sums are exact and independent of the order of the
+// additions: the totals are deterministic, need no sort, and are at least as accurate as the
+// reference's sequential double sums (they are rounded once, when converted back).
+struct Fx {
+    uint64_t hi, lo;
+};
+__device__ __forceinline__ Fx fx_from(double c) {
+    const double s = c * 1048576.0;  // 2^20
+    const double h = floor(s);
+    return Fx{static_cast<uint64_t>(h), __double2ull_rz((s - h) * 18446744073709551616.0)};  // x 2^64
+}
+__device__ __forceinline__ Fx fx_add(Fx a, Fx b) {
+    Fx r;
+    r.lo = a.lo + b.lo;
+    r.hi = a.hi + b.hi + (r.lo < a.lo ? 1ull : 0ull);
+    return r;
+}
+__device__ __forceinline__ double fx_double(Fx a) {
+    return static_cast<double>(a.hi) * 9.5367431640625e-07 + static_cast<double>(a.lo) * 5.169878828456423e-26;
+}
+__device__ __forceinline__ Fx fx_shfl_up(Fx a, int d) {
+    return Fx{__shfl_up_sync(0xffffffffu, a.hi, d), __shfl_up_sync(0xffffffffu, a.lo, d)};
+}
+__device__ __forceinline__ Fx fx_shfl_xor(Fx a, int d) {
+    return Fx{__shfl_xor_sync(0xffffffffu, a.hi, d), __shfl_xor_sync(0xffffffffu, a.lo, d)};
+}
+__device__ __forceinline__ Fx fx_warp_incl(Fx v, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const Fx o = fx_shfl_up(v, d);
+        if (lane >= d) v = fx_add(o, v);
+    }
+    return v;
+}
+__device__ __forceinline__ Fx fx_warp_sum(Fx v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v = fx_add(v, fx_shfl_xor(v, d));
+    return v;
+}
+
+struct FxContribution {
+    Fx mit, cfd;
+    uint64_t occ;
+};
+
+// r: seg record (position, slice, site id, occurrences), sig: the site's signature
+__device__ __forceinline__ FxContribution fx_contribution(const ScoreArgs& a, const Tables& T, uint64_t q, const uint4& r,
+                                                         uint64_t sig) {
+    const Contribution c = contribution(T, a.P, q, sig, r.w);
+    return FxContribution{fx_from(c.mit), fx_from(c.cfd), c.occ};
+}
+
+constexpr int kWarpSort = 1024;  // exiting guides with more hits are ordered by a whole block
+
+// Warp per guide, pass 1: every hit's contribution added exactly. If the method's test does not
+// fire on the totals it never fires on a prefix (contributions are >= 0 and the tests are
+// monotone), so the totals are the reference's result and no ordering is needed; guides whose
+// test fires go to the ordered scorers.
+__global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t* keys = s_keys[warp];
     const Tables& T = *a.tables;
     if (a.counters->overflow) return;  // rerun follows
     const uint64_t gw = blockIdx.x * 8ull + warp, nw = gridDim.x * 8ull;
     for (uint64_t qi = gw; qi < a.n; qi += nw) {
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
-        if (L > static_cast<uint32_t>(kWarpHits)) {
-            if (lane == 0) a.big[atomicAdd(&a.counters->n_big, 1u)] = static_cast<uint32_t>(qi);
-            continue;
-        }
         const uint64_t q = a.qsig[qi];
         const uint4* seg = a.seg + h0;
-        uint32_t P2 = 1;
-        while (P2 < L) P2 <<= 1;
-        for (uint32_t i = lane; i < P2; i += 32)
-            keys[i] = i < L ? (order_key(seg[i]) << 8) | i : ~0ull;
+        const uint64_t* sig = a.segsig + h0;
+        Fx tm{0, 0}, tc{0, 0};
+        uint64_t tn = 0;
+        for (uint32_t i = lane; i < L; i += 32) {
+            const FxContribution c = fx_contribution(a, T, q, seg[i], sig[i]);
+            tm = fx_add(tm, c.mit);
+            tc = fx_add(tc, c.cfd);
+            tn += c.occ;
+        }
+        tm = fx_warp_sum(tm);
+        tc = fx_warp_sum(tc);
+        for (int d = 16; d > 0; d >>= 1) tn += __shfl_xor_sync(0xffffffffu, tn, d);
+        if (exit_test(a.P, fx_double(tm), fx_double(tc))) {
+            if (lane == 0) {
+                if (L <= static_cast<uint32_t>(kWarpSort))
+                    a.exitq[atomicAdd(&a.counters->n_exit, 1u)] = static_cast<uint32_t>(qi);
+                else
+                    a.big[atomicAdd(&a.counters->n_big, 1u)] = static_cast<uint32_t>(qi);
+            }
+            continue;
+        }
+        if (a.P.want_distinct)
+            for (uint32_t i = lane; i < L; i += 32) {
+                const uint32_t id = seg[i].z;
+                atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+            }
+        if (lane == 0)
+            finalise(a.P, fx_double(tm), fx_double(tc), tn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+    }
+}
+
+// Warp per guide whose test fires (at most kWarpSort hits). The reference visits hits by slice,
+// then list position. The hits are first bucketed by slice (counting sort); whole slices are
+// added exactly while the running totals do not fire the test -- within a slice the order then
+// does not matter -- and only the slice where the test fires is sorted by list position (a
+// bitonic network whose comparators all point the same way; missing elements act as +infinity)
+// to find the exact hit where the reference stops. Scores and counts are those at that hit.
+struct OrderedSmem {
+    uint64_t keys[kWarpSort];
+    uint16_t idx[kWarpSort];
+    uint32_t cnt[kMaxSlices + 1];
+    uint32_t cur[kMaxSlices];
+};
+
+__global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
+    extern __shared__ __align__(16) uint8_t s_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    OrderedSmem& W = reinterpret_cast<OrderedSmem*>(s_raw)[warp];
+    const Tables& T = *a.tables;
+    if (a.counters->overflow) return;  // rerun follows
+    const uint32_t S = a.ix.n_slices;
+    const uint32_t n_exit = a.counters->n_exit;
+    const uint32_t gw = blockIdx.x * 8 + warp, nw = gridDim.x * 8;
+    for (uint32_t e = gw; e < n_exit; e += nw) {
+        const uint64_t qi = a.exitq[e];
+        const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
+        const uint64_t q = a.qsig[qi];
+        const uint4* seg = a.seg + h0;
+        const uint64_t* sig = a.segsig + h0;
+        // counting sort of the hits by slice
+        for (uint32_t t = lane; t <= S; t += 32) W.cnt[t] = 0;
         __syncwarp();
-        for (uint32_t k = 2; k <= P2; k <<= 1) {
-            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                for (uint32_t i = lane; i < P2; i += 32) {
-                    // first stage of each merge compares mirrored pairs, later stages i / i+j
-                    const uint32_t partner = (j == (k >> 1)) ? (i ^ (k - 1)) : (i ^ j);
-                    if (partner > i) {
-                        const uint64_t x = keys[i], y = keys[partner];
-                        if (x > y) {
-                            keys[i] = y;
-                            keys[partner] = x;
+        for (uint32_t i = lane; i < L; i += 32) atomicAdd(&W.cnt[seg[i].y], 1u);
+        __syncwarp();
+        if (lane == 0) {
+            uint32_t acc = 0;
+            for (uint32_t t = 0; t < S; t++) {
+                const uint32_t c = W.cnt[t];
+                W.cnt[t] = acc;
+                W.cur[t] = acc;
+                acc += c;
+            }
+            W.cnt[S] = acc;
+        }
+        __syncwarp();
+        for (uint32_t i = lane; i < L; i += 32) W.idx[atomicAdd(&W.cur[seg[i].y], 1u)] = static_cast<uint16_t>(i);
+        __syncwarp();
+        Fx rm{0, 0}, rc{0, 0};
+        uint64_t rn = 0;
+        bool stopped = false;
+        for (uint32_t sl = 0; sl < S && !stopped; sl++) {
+            const uint32_t b0 = W.cnt[sl], ns = W.cnt[sl + 1] - b0;
+            if (!ns) continue;
+            Fx tm{0, 0}, tc{0, 0};
+            uint64_t tn = 0;
+            for (uint32_t j = lane; j < ns; j += 32) {
+                const uint32_t h = W.idx[b0 + j];
+                const FxContribution c = fx_contribution(a, T, q, seg[h], sig[h]);
+                tm = fx_add(tm, c.mit);
+                tc = fx_add(tc, c.cfd);
+                tn += c.occ;
+            }
+            tm = fx_add(fx_warp_sum(tm), rm);
+            tc = fx_add(fx_warp_sum(tc), rc);
+            for (int d = 16; d > 0; d >>= 1) tn += __shfl_xor_sync(0xffffffffu, tn, d);
+            if (!exit_test(a.P, fx_double(tm), fx_double(tc))) {
+                if (a.P.want_distinct)
+                    for (uint32_t j = lane; j < ns; j += 32) {
+                        const uint32_t id = seg[W.idx[b0 + j]].z;
+                        atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                    }
+                rm = tm;
+                rc = tc;
+                rn += tn;
+                continue;
+            }
+            // the test fires inside this slice: order its hits by list position
+            uint32_t P2 = 1;
+            while (P2 < ns) P2 <<= 1;
+            for (uint32_t j = lane; j < P2; j += 32)
+                W.keys[j] = j < ns ? (static_cast<uint64_t>(seg[W.idx[b0 + j]].x) << 10) | W.idx[b0 + j] : ~0ull;
+            __syncwarp();
+            for (uint32_t k = 2; k <= P2; k <<= 1) {
+                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                    for (uint32_t i = lane; i < P2; i += 32) {
+                        // first stage of each merge compares mirrored pairs, later stages i / i+j
+                        const uint32_t partner = (j == (k >> 1)) ? (i ^ (k - 1)) : (i ^ j);
+                        if (partner > i) {
+                            const uint64_t x = W.keys[i], y = W.keys[partner];
+                            if (x > y) {
+                                W.keys[i] = y;
+                                W.keys[partner] = x;
+                            }
                         }
                     }
+                    __syncwarp();
                 }
-                __syncwarp();
             }
-        }
-        double run_mit = 0.0, run_cfd = 0.0;
-        uint64_t run_cnt = 0;
-        bool stopped = false;
-        for (uint32_t c0 = 0; c0 < L && !stopped; c0 += 32) {
-            const uint32_t t = c0 + lane;
-            Contribution c{0.0, 0.0, 0};
-            uint32_t id = 0;
-            if (t < L) {
-                const uint4 r = seg[keys[t] & 0xFF];
-                id = r.w;
-                const uint4 sr = a.ix.srec[id];  // signature and occurrences in one read
-                c = contribution(T, a.P, q, (static_cast<uint64_t>(sr.y) << 32) | sr.x, sr.z);
+            for (uint32_t c0 = 0; c0 < ns && !stopped; c0 += 32) {
+                const uint32_t t = c0 + lane;
+                FxContribution c{{0, 0}, {0, 0}, 0};
+                uint32_t id = 0;
+                if (t < ns) {
+                    const uint32_t h = W.keys[t] & 1023u;
+                    const uint4 r = seg[h];
+                    id = r.z;
+                    c = fx_contribution(a, T, q, r, sig[h]);
+                }
+                const Fx im = fx_add(fx_warp_incl(c.mit, lane), rm);
+                const Fx ic = fx_add(fx_warp_incl(c.cfd, lane), rc);
+                const uint64_t in = warp_incl_sum_u64(c.occ, lane) + rn;
+                const bool ex = t < ns && exit_test(a.P, fx_double(im), fx_double(ic));
+                const unsigned em = __ballot_sync(0xffffffffu, ex);
+                const int last = em ? __ffs(em) - 1 : (ns - c0 >= 32 ? 31 : static_cast<int>(ns - c0 - 1));
+                if (a.P.want_distinct && t < ns && lane <= last) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                rm = Fx{__shfl_sync(0xffffffffu, im.hi, last), __shfl_sync(0xffffffffu, im.lo, last)};
+                rc = Fx{__shfl_sync(0xffffffffu, ic.hi, last), __shfl_sync(0xffffffffu, ic.lo, last)};
+                rn = __shfl_sync(0xffffffffu, in, last);
+                stopped = em != 0;
             }
-            const double im = warp_incl_sum(c.mit, lane) + run_mit;
-            const double ic = warp_incl_sum(c.cfd, lane) + run_cfd;
-            const uint64_t in = warp_incl_sum_u64(c.occ, lane) + run_cnt;
-            const bool ex = t < L && exit_test(a.P, im, ic);
-            const unsigned em = __ballot_sync(0xffffffffu, ex);
-            const int last = em ? __ffs(em) - 1 : (L - c0 >= 32 ? 31 : static_cast<int>(L - c0 - 1));
-            if (a.P.want_distinct && t < L && lane <= last) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
-            run_mit = __shfl_sync(0xffffffffu, im, last);
-            run_cfd = __shfl_sync(0xffffffffu, ic, last);
-            run_cnt = __shfl_sync(0xffffffffu, in, last);
-            stopped = em != 0;
+            __syncwarp();
         }
-        if (lane == 0)
-            finalise(a.P, run_mit, run_cfd, run_cnt, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+        if (lane == 0) finalise(a.P, fx_double(rm), fx_double(rc), rn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
         __syncwarp();
     }
 }
 
-// Block per guide with more than kWarpHits hits. Up to kBlockHits hits are sorted in shared
-// memory (keys with the hit index in the low bits); larger segments are sorted in place in
-// global memory. Both use the same one-direction bitonic network as the warp path, then the
-// ordered accumulation runs with block-wide prefix sums.
+// Block per guide whose test fires and that has more than kWarpSort hits: up to kBlockHits hits
+// are sorted in shared memory, larger segments in place in global memory, then the ordered
+// accumulation runs with exact block-wide prefix sums.
 constexpr int kBlockHits = 8192;
 constexpr int kBlockIdxBits = 13;
 
 __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
     extern __shared__ __align__(16) uint64_t s_bkeys[];  // kBlockHits keys
-    __shared__ SliceGeom s_geom[kMaxSlices];
-    __shared__ double s_wm[8], s_wc[8];
+    __shared__ Fx s_wm[8], s_wc[8];
     __shared__ uint64_t s_wn[8];
     __shared__ int s_first;
-    for (int i = threadIdx.x; i < static_cast<int>(a.ix.n_slices); i += blockDim.x) s_geom[i] = a.ix.geom[i];
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const Tables& T = *a.tables;
     if (a.counters->overflow) return;  // rerun follows
@@ -806,6 +965,7 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
         const uint64_t qi = a.big[b];
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         uint4* seg = a.seg + h0;
+        uint64_t* sig = a.segsig + h0;
         const uint64_t q = a.qsig[qi];
         uint32_t P2 = 1;
         while (P2 < L) P2 <<= 1;
@@ -818,7 +978,6 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
         for (uint32_t k = 2; k <= P2; k <<= 1) {
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
                 for (uint32_t i = threadIdx.x; i < P2; i += blockDim.x) {
-                    // first stage of each merge compares mirrored pairs, later stages i / i+j
                     const uint32_t partner = (j == (k >> 1)) ? (i ^ (k - 1)) : (i ^ j);
                     if (partner <= i) continue;
                     if (in_smem) {
@@ -832,26 +991,29 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
                         if (order_key(x) > order_key(y)) {
                             seg[i] = y;
                             seg[partner] = x;
+                            const uint64_t sx = sig[i];
+                            sig[i] = sig[partner];
+                            sig[partner] = sx;
                         }
                     }
                 }
                 __syncthreads();
             }
         }
-        double run_mit = 0.0, run_cfd = 0.0;
-        uint64_t run_cnt = 0;
+        Fx run_m{0, 0}, run_c{0, 0};
+        uint64_t run_n = 0;
         bool stopped = false;
         for (uint32_t c0 = 0; c0 < L && !stopped; c0 += blockDim.x) {
             const uint32_t t = c0 + threadIdx.x;
-            Contribution c{0.0, 0.0, 0};
+            FxContribution c{{0, 0}, {0, 0}, 0};
             uint32_t id = 0;
             if (t < L) {
-                const uint4 r = in_smem ? seg[s_bkeys[t] & ((1u << kBlockIdxBits) - 1)] : seg[t];
-                id = r.w;
-                const uint4 sr = a.ix.srec[id];
-                c = contribution(T, a.P, q, (static_cast<uint64_t>(sr.y) << 32) | sr.x, sr.z);
+                const uint32_t h = in_smem ? static_cast<uint32_t>(s_bkeys[t] & ((1u << kBlockIdxBits) - 1)) : t;
+                const uint4 r = seg[h];
+                id = r.z;
+                c = fx_contribution(a, T, q, r, sig[h]);
             }
-            double im = warp_incl_sum(c.mit, lane), ic = warp_incl_sum(c.cfd, lane);
+            Fx im = fx_warp_incl(c.mit, lane), ic = fx_warp_incl(c.cfd, lane);
             uint64_t in = warp_incl_sum_u64(c.occ, lane);
             if (lane == 31) {
                 s_wm[warp] = im;
@@ -860,17 +1022,17 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             }
             if (threadIdx.x == 0) s_first = 0x7fffffff;
             __syncthreads();
-            double pm = run_mit, pc = run_cfd;
-            uint64_t pn = run_cnt;
+            Fx pm = run_m, pc = run_c;
+            uint64_t pn = run_n;
             for (int w = 0; w < warp; w++) {
-                pm += s_wm[w];
-                pc += s_wc[w];
+                pm = fx_add(pm, s_wm[w]);
+                pc = fx_add(pc, s_wc[w]);
                 pn += s_wn[w];
             }
-            im += pm;
-            ic += pc;
+            im = fx_add(im, pm);
+            ic = fx_add(ic, pc);
             in += pn;
-            if (t < L && exit_test(a.P, im, ic)) atomicMin(&s_first, static_cast<int>(threadIdx.x));
+            if (t < L && exit_test(a.P, fx_double(im), fx_double(ic))) atomicMin(&s_first, static_cast<int>(threadIdx.x));
             __syncthreads();
             const int first = s_first;
             const uint32_t in_chunk = L - c0 < blockDim.x ? L - c0 : blockDim.x;
@@ -884,14 +1046,14 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
                 s_wn[0] = in;
             }
             __syncthreads();
-            run_mit = s_wm[0];
-            run_cfd = s_wc[0];
-            run_cnt = s_wn[0];
+            run_m = s_wm[0];
+            run_c = s_wc[0];
+            run_n = s_wn[0];
             stopped = first != 0x7fffffff;
             __syncthreads();
         }
         if (threadIdx.x == 0)
-            finalise(a.P, run_mit, run_cfd, run_cnt, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+            finalise(a.P, fx_double(run_m), fx_double(run_c), run_n, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
         __syncthreads();
     }
 }
@@ -961,6 +1123,8 @@ Workspace& workspace(issl_index* ix) {
         ISSL_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, ws->scan_smem));
         ISSL_CUDA(cudaFuncSetAttribute(k_score_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(kBlockHits * sizeof(uint64_t))));
+        ISSL_CUDA(cudaFuncSetAttribute(k_score_ordered, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(8 * sizeof(OrderedSmem))));
         ISSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kScanWarps * 32, ws->scan_smem));
         ws->scan_blocks = sm_count(ix->device) * std::max(per_sm, 1);
         ws->counters.reserve(1);
@@ -988,6 +1152,7 @@ void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, cudaStream_t st) {
         ws.qhits.reserve(cap + 1);
         ws.qhoff.reserve(cap + 1);
         ws.big.reserve(cap);
+        ws.exitq.reserve(cap);
         ws.out_mit.reserve(cap);
         ws.out_cfd.reserve(cap);
         ws.out_code.reserve(cap);
@@ -1013,6 +1178,7 @@ void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, cudaStream_t st) {
     if (ws.cand_cap < want_cands) {
         ws.cands.reserve(want_cands);
         ws.seg.reserve(want_cands);
+        ws.segsig.reserve(want_cands);
         ws.cand_cap = want_cands;
     }
 }
@@ -1081,13 +1247,15 @@ void enqueue_pipeline(issl_index* ix, Workspace& ws, const uint64_t* d_qsig, uin
     k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, v, ws.qhits.p);
     device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, nullptr, n, ws.scan32.p,
                                  ws.qhoff.p + n, st);
-    k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, ws.qhits.p, ws.qhoff.p, ix->ids.p,
-                                           ix->n_sites, ws.seg.p);
+    k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, ws.qhits.p, ws.qhoff.p, v, ws.seg.p,
+                                           ws.segsig.p);
     if (P.want_distinct) ISSL_CUDA(cudaMemsetAsync(ws.bitmap.p, 0, (ix->n_sites / 32 + 1) * 4, st));
     ScoreArgs a;
     a.ix = v;
     a.qsig = d_qsig;
     a.seg = ws.seg.p;
+    a.segsig = ws.segsig.p;
+    a.exitq = ws.exitq.p;
     a.qhoff = ws.qhoff.p;
     a.tables = ws.tables.p;
     a.counters = ws.counters.p;
@@ -1099,15 +1267,16 @@ void enqueue_pipeline(issl_index* ix, Workspace& ws, const uint64_t* d_qsig, uin
     a.out_cfd = d_cfd;
     a.out_code = d_code;
     a.out_count = d_count;
-    k_score_warp<<<grid_for(n, 8, sms * 8), 256, 0, st>>>(a);
+    k_score_sum<<<grid_for(n, 8, sms * 8), 256, 0, st>>>(a);
+    k_score_ordered<<<sms * 4, 256, 8 * sizeof(OrderedSmem), st>>>(a);
     k_score_block<<<sms * 2, 256, kBlockHits * sizeof(uint64_t), st>>>(a);
     if (P.want_distinct) k_popcount<<<sms * 4, 256, 0, st>>>(ws.bitmap.p, ix->n_sites / 32 + 1, ws.counters.p);
     ISSL_CUDA(cudaEventRecord(ws.ev[3], st));
     ISSL_CUDA(cudaGetLastError());
     // probe_count, 3 bucket-scan, units_finalize, bucket_stats, probe_scatter, scan,
-    // cands_finalize, cand_own, 3 hit-offset scan, hit_scatter, score_warp, score_block
-    // (+ popcount for distinct counts)
-    ws.launches += 16 + (P.want_distinct ? 1 : 0);
+    // cands_finalize, cand_own, 3 hit-offset scan, hit_scatter, score_sum, score_ordered,
+    // score_block (+ popcount for distinct counts)
+    ws.launches += 17 + (P.want_distinct ? 1 : 0);
 }
 
 // Reads the counters after a pipeline run; returns false (and grows capacities) on overflow.
@@ -1134,6 +1303,7 @@ bool check_and_grow(issl_index* ix, Workspace& ws, uint64_t n, cudaStream_t st) 
                      "more than 2^32 candidate sites in one call; split the guides");
         ws.cands.reserve(cap);
         ws.seg.reserve(cap);
+        ws.segsig.reserve(cap);
         ws.cand_cap = cap;
         ok = false;
     }
