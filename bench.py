@@ -68,6 +68,7 @@ def parse():
     ap.add_argument("--queries", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default scan tuning (no autotune sweep)")
     return ap.parse_args()
 
 
@@ -219,6 +220,14 @@ def run_ours(args):
         ix.score_device(d_q.data_ptr(), nq, method_id, thr, md, d_mit.data_ptr(), d_cfd.data_ptr(),
                         d_code.data_ptr(), d_cnt.data_ptr(), d_dist.data_ptr(), stream.cuda_stream)
 
+    # ---- scan tuning: swept on this workload's own guides before any timing -----------------
+    tuning = None
+    if not args.no_tune:
+        t, rep = ix.autotune(d_q.data_ptr(), nq, method_id, thr, md)
+        tuning = {"chunk": list(t.chunk), "stages": t.stages, "blocks_per_sm": t.blocks_per_sm,
+                  "default_ms": rep.default_ms, "tuned_ms": rep.best_ms, "configs_timed": rep.configs_timed,
+                  "class_probes": list(rep.class_probes)}
+
     # ---- device-resident throughput -------------------------------------------------------
     scan_ms, scan_bytes, launches = [], [], 0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -306,6 +315,8 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "probes_per_s": value * len(__import__("cracklingplusplus_gpu_b200").slice_masks(WORKLOAD["slice_config"])),
+        "owned_hits_per_step": int(ix.last_stats().hits),
+        "tuning": tuning,
         "generation_s": gen_s,
     }
     if rank == 0 and world == 1 and not args.no_cpu:

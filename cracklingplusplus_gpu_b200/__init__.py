@@ -11,6 +11,11 @@ Python mirrors of the reference's interfaces:
   * ``ISSLScoringModule``  -- same constructor/run() contract as include/ISSLScoringModule.hpp:15-29
                               (drives the C++ drop-in class through ``issl_module_run``)
   * ``OT_METHODS`` / ``CLI_METHODS`` -- otScoreMethod numbering and the CLI's method words
+
+Beyond the reference: ``Batch`` scores many guide sets (each with its own method, threshold and
+mismatch bound) in one graph-captured pass; ``Index.autotune`` sweeps the scan's tile and staging
+parameters per bucket-size class; ``Server`` admits guide-set requests by device-memory footprint
+and scores them with continuous batching over several in-flight slots.
 """
 from __future__ import annotations
 
@@ -21,6 +26,8 @@ from ._lib import (  # noqa: F401
     lib,
     library_path,
 )
+from .batch import Batch  # noqa: F401
 from .index import Index, ScoreResult, SynthSpec, tables  # noqa: F401
 from .module import CracklingConfig, GuideResults, ISSLScoringModule  # noqa: F401
+from .server import Server  # noqa: F401
 from .slice_configs import SLICE_CONFIGS, slice_masks  # noqa: F401

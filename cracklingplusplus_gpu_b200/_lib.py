@@ -33,7 +33,45 @@ class IndexInfo(C.Structure):
 class ScoreStats(C.Structure):
     _fields_ = [("scan_ms", C.c_double), ("total_ms", C.c_double), ("probes", C.c_uint64),
                 ("buckets_scanned", C.c_uint64), ("entries_scanned", C.c_uint64), ("units", C.c_uint64),
-                ("hits", C.c_uint64), ("scan_bytes", C.c_uint64), ("launches", C.c_uint64)]
+                ("hits", C.c_uint64), ("scan_bytes", C.c_uint64), ("launches", C.c_uint64),
+                ("class_probes", C.c_uint64 * 3), ("candidates", C.c_uint64)]
+
+
+class Tuning(C.Structure):
+    """issl_tuning: scan unit size per bucket-size class (<64, 64..4095, >=4096 entries),
+    staging depth, scan blocks per SM (0 = as many as fit)."""
+    _fields_ = [("chunk", C.c_uint32 * 3), ("stages", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
+
+    def as_tuple(self):
+        return (tuple(self.chunk), self.stages, self.blocks_per_sm)
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("default_ms", C.c_double), ("best_ms", C.c_double), ("configs_timed", C.c_uint32),
+                ("from_cache", C.c_uint32), ("class_probes", C.c_uint64 * 3)]
+
+
+class ServerConfig(C.Structure):
+    """issl_server_config (zeros select the defaults: 3 slots, 131072 guides per batch, 16 GiB headroom)."""
+    _fields_ = [("n_slots", C.c_uint32), ("max_wait_us", C.c_uint32), ("max_batch_guides", C.c_uint64),
+                ("headroom_bytes", C.c_uint64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("service_ms", C.c_double), ("latency_ms", C.c_double),
+                ("batch_guides", C.c_uint64), ("batch_requests", C.c_uint32), ("slot", C.c_uint32)]
+
+
+class ServerSummary(C.Structure):
+    _fields_ = [("requests", C.c_uint64), ("guides", C.c_uint64), ("batches", C.c_uint64), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("max_ms", C.c_double), ("mean_batch_guides", C.c_double),
+                ("slots", C.c_uint32), ("peak_in_flight", C.c_uint32), ("slot_budget_bytes", C.c_uint64),
+                ("peak_batch_bytes", C.c_uint64)]
+
+
+class GuideSet(C.Structure):
+    """issl_guide_set: one set of a batch (consecutive guides sharing method/threshold/max_dist)."""
+    _fields_ = [("count", C.c_uint64), ("method", C.c_int), ("max_dist", C.c_int), ("threshold", C.c_double)]
 
 
 class SynthSpecC(C.Structure):
@@ -71,6 +109,22 @@ SIGNATURES = [
     ("issl_score_device", C.c_int, [vp, vp, C.c_size_t, C.c_int, C.c_double, C.c_int, vp, vp, vp, vp, vp, vp]),
     ("issl_score_device_static", C.c_int, [vp, vp, C.c_size_t, C.c_int, C.c_double, C.c_int, vp, vp, vp, vp, vp]),
     ("issl_last_stats", C.c_int, [vp, P(ScoreStats)]),
+    ("issl_get_tuning", C.c_int, [vp, P(Tuning)]),
+    ("issl_set_tuning", C.c_int, [vp, P(Tuning)]),
+    ("issl_autotune", C.c_int, [vp, vp, C.c_size_t, C.c_int, C.c_double, C.c_int, C.c_char_p, P(Tuning),
+                                P(TuneReport)]),
+    ("issl_batch_create", C.c_int, [vp, P(vp)]),
+    ("issl_batch_destroy", None, [vp]),
+    ("issl_batch_score", C.c_int, [vp, vp, C.c_size_t, P(GuideSet), C.c_size_t, vp, vp, vp, vp, vp]),
+    ("issl_batch_score_host", C.c_int, [vp, u64p, C.c_size_t, P(GuideSet), C.c_size_t, f64p, f64p, C.c_char_p,
+                                        u64p]),
+    ("issl_batch_stats", C.c_int, [vp, P(ScoreStats)]),
+    ("issl_workspace_bytes", C.c_int, [vp, C.c_uint64, C.c_double, u64p]),
+    ("issl_server_create", C.c_int, [vp, P(ServerConfig), P(vp)]),
+    ("issl_server_submit", C.c_int, [vp, u64p, C.c_size_t, C.c_int, C.c_double, C.c_int, u64p]),
+    ("issl_server_wait", C.c_int, [vp, C.c_uint64, C.c_int, f64p, f64p, C.c_char_p, u64p, P(RequestInfo)]),
+    ("issl_server_stats", C.c_int, [vp, P(ServerSummary), C.c_int]),
+    ("issl_server_destroy", None, [vp]),
     ("issl_synth", C.c_int, [P(SynthSpecC), C.c_int, P(vp), u64p]),
     ("issl_tables", C.c_int, [u64p, f64p, f64p, f64p]),
     ("issl_module_run", C.c_int, [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_size_t,

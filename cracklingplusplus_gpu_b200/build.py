@@ -17,7 +17,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libissl_b200.so")
 CLI = os.path.join(HERE, "issl_score_offtargets")
-SOURCES = ["index.cu", "score.cu", "radix_sort.cu", "synth.cu", "tables.cpp", "module.cpp"]
+SOURCES = ["index.cu", "score.cu", "radix_sort.cu", "synth.cu", "tables.cpp", "module.cpp", "tune.cpp", "serve.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -139,6 +139,9 @@ struct issl_index {
     issl::DevBuf<issl::SliceGeom> d_geom;
     std::unique_ptr<issl::Workspace> ws;
     issl_score_stats stats{};
+    // scan unit size per bucket-size class, staging depth, blocks per SM (issl_set_tuning)
+    issl_tuning tuning{{1024, 1024, 1024}, 3, 0};
+    uint32_t tuning_version = 0;
     issl::IndexView view() const;
     issl_index();  // defined where Workspace is complete
     ~issl_index();
@@ -158,6 +161,9 @@ void radix_sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, ui
 void radix_sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp,
                           size_t n, int bits, void* temp, size_t temp_bytes, cudaStream_t st,
                           uint64_t** keys_out, uint32_t** vals_out);
+
+// device bytes of a scoring workspace: fixed + n * per_guide + candidates * per_candidate (score.cu)
+void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide, uint64_t* per_candidate);
 
 // tables (tables.cpp)
 const std::vector<double>& mit_rank_table();   // 6195 entries indexed by subset rank

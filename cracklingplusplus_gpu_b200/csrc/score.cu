@@ -36,7 +36,7 @@
 
 namespace issl {
 
-constexpr int kChunk = 1024;       // list positions per scan unit: 32 bit-sliced blocks of 32
+constexpr int kChunk = 1024;       // largest scan unit: 32 bit-sliced blocks of 32 list positions
 constexpr int kGroup = 32;         // guides per scan unit
 constexpr int kScanWarps = 4;      // warps per scan block
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
@@ -58,11 +58,13 @@ struct Counters {
     uint32_t n_big;         // exiting guides with more than kWarpSort hits (block scorer)
     uint32_t n_exit;        // exiting guides with at most kWarpSort hits (warp scorer)
     uint32_t overflow;      // 1: units, 2: hits, 4: a bounded wait in the scan gave up
+    uint32_t next_batch;    // work queue of the scan: next batch of 32 units to take
     uint32_t pad;
     uint64_t distinct;
     uint64_t buckets;       // distinct buckets probed
     uint64_t entries;       // entries compared by the scan (per guide group)
     uint64_t rbytes;        // bit-sliced bytes the scan copies
+    uint64_t class_probes[3];  // probes into buckets of < 64, 64..4095, >= 4096 entries
 };
 
 struct Tables {  // device copies of the penalty tables
@@ -79,9 +81,31 @@ struct ScoreParams {
     double threshold;
     double maximum_sum;  // (10000 - 100 t) / t, ISSLScoringModule.cpp:225
     int want_distinct;
+    int pad;
 };
 
-constexpr int kStages = 3;
+// A batch of guide sets scored in one pass: the header and the set table live in device memory
+// so that a captured graph can be replayed for any batch that fits the capacities.
+struct SetDesc {
+    ScoreParams P;
+    uint32_t begin, count;  // the set's guides: [begin, begin + count) of the batch
+};
+struct BatchHeader {
+    uint32_t n;         // guides in the batch
+    uint32_t n_sets;
+    int max_dist;       // largest max_dist of the sets (the scan's bound)
+    uint32_t pad;
+};
+
+// Unit size per bucket-size class (autotuned per index).
+struct ChunkClasses {
+    uint32_t c[3];  // list positions per unit for buckets of < 64, 64..4095 and >= 4096 entries
+};
+__device__ __forceinline__ uint64_t chunk_of(uint64_t bucket_size, const ChunkClasses& cc) {
+    return bucket_size < 64 ? cc.c[0] : bucket_size < 4096 ? cc.c[1] : cc.c[2];
+}
+
+constexpr int kMaxStages = 4;
 constexpr int kStageQr = kGroup + 2;     // (guide, residual) pairs per stage + alignment slack
 constexpr uint32_t kCandSlab = 256;
 constexpr uint32_t kDeadCand = 0xFFFFFFFFu;  // guide field of an unused or rejected candidate slot
@@ -99,20 +123,22 @@ struct StageMeta {
     uint32_t delta;// words between the 16-byte aligned copy start and the unit's first block
 };
 
-// per-warp shared memory, sized at launch for the widest block of the index
+// per-warp shared memory, sized at launch for the widest block of the index and the stage count
 struct WarpLayout {
+    uint32_t stages;
     uint32_t stage_words;  // 32 blocks x words per block (largest slice)
     uint32_t qr_off, qm_off, meta_off, bar_off, bytes;
 };
 
-__host__ __device__ inline WarpLayout warp_layout(uint32_t max_wpb) {
+__host__ __device__ inline WarpLayout warp_layout(uint32_t max_wpb, uint32_t stages) {
     WarpLayout L;
+    L.stages = stages;
     L.stage_words = (32u * max_wpb + 3u + 3u) & ~3u;  // 32 blocks + alignment slack, 16-byte multiple
-    L.qr_off = kStages * L.stage_words * 4u;                 // 16-byte aligned (stage_words % 4 == 0)
-    L.qm_off = L.qr_off + kStages * kStageQr * 8u;
+    L.qr_off = stages * L.stage_words * 4u;                 // 16-byte aligned (stage_words % 4 == 0)
+    L.qm_off = L.qr_off + stages * kStageQr * 8u;
     L.meta_off = L.qm_off + 32u * 4u;
-    L.bar_off = L.meta_off + kStages * static_cast<uint32_t>(sizeof(StageMeta));
-    L.bytes = (L.bar_off + kStages * 8u + 15u) & ~15u;
+    L.bar_off = L.meta_off + stages * static_cast<uint32_t>(sizeof(StageMeta));
+    L.bytes = (L.bar_off + stages * 8u + 15u) & ~15u;
     return L;
 }
 
@@ -149,10 +175,26 @@ struct issl::Workspace {
     DevBuf<uint64_t> out_count, out_distinct;
     Counters last{};
     uint64_t launches = 0;  // kernels enqueued by the current call
+    uint32_t tuning_version = ~0u;  // version of the index's tuning the scan is configured for
+    uint64_t epoch = 0;             // bumped whenever a buffer is reallocated
+    // batch form: set table (header + sets) on the device and its pinned host staging, the
+    // guide -> set map, and the captured pipeline
+    DevBuf<uint16_t> qset;
+    DevBuf<uint8_t> batch;
+    uint8_t* h_batch = nullptr;
+    size_t sets_cap = 0;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_epoch = ~0ull;
+    uint32_t graph_tuning = ~0u;
+    uint64_t graph_kernels = 0;
     ~Workspace() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (h_batch) cudaFreeHost(h_batch);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (own_stream) cudaStreamDestroy(own_stream);
+        if (cap_stream) cudaStreamDestroy(cap_stream);
     }
 };
 
@@ -179,13 +221,16 @@ __global__ void k_encode_ascii(const char* __restrict__ ascii, size_t stride, ui
     }
 }
 
-__global__ void k_probe_count(IndexView ix, const uint64_t* __restrict__ qsig, uint64_t n,
+// n: guides, or *d_n when the count lives on the device (batch form)
+__device__ __forceinline__ uint64_t guide_count(const uint32_t* d_n, uint64_t n) { return d_n ? *d_n : n; }
+
+__global__ void k_probe_count(IndexView ix, const uint64_t* __restrict__ qsig, const uint32_t* d_n, uint64_t n,
                               uint32_t* __restrict__ probe_gb, uint32_t* __restrict__ bucket_cnt,
                               const uint64_t* __restrict__ off) {
     __shared__ SliceGeom g[kMaxSlices];
     for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
     __syncthreads();
-    const uint64_t S = ix.n_slices, total = n * S;
+    const uint64_t S = ix.n_slices, total = guide_count(d_n, n) * S;
     for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < total;
          p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint64_t q = p / S;
@@ -202,12 +247,15 @@ struct BucketLoad {
     const uint32_t* cnt;
     const uint64_t* off;
     uint64_t n_sites;
+    ChunkClasses cc;
     __device__ uint64_t operator()(uint64_t g) const {
         const uint32_t c = cnt[g];
         if (!c) return 0;
-        // chunks are aligned to kChunk list positions of the slice, so a unit never spans two
+        // chunks are aligned to the chunk size within the slice (which divides kChunk), so a
+        // unit never spans two kChunk blocks
+        const uint64_t C = chunk_of(off[g + 1] - off[g], cc);
         const uint64_t sb = (off[g] / n_sites) * n_sites;
-        const uint64_t chunks = (off[g + 1] - 1 - sb) / kChunk - (off[g] - sb) / kChunk + 1;
+        const uint64_t chunks = (off[g + 1] - 1 - sb) / C - (off[g] - sb) / C + 1;
         const uint64_t units = chunks * ((c + kGroup - 1) / kGroup);
         return (units << 32) | c;
     }
@@ -220,6 +268,7 @@ struct BucketStore {
     UnitDesc* units;
     uint64_t unit_cap;
     uint64_t n_sites;
+    ChunkClasses cc;
     __device__ void operator()(uint64_t g, uint64_t ex, uint64_t inc) const {
         qstart[g] = static_cast<uint32_t>(ex);
         const uint32_t c = static_cast<uint32_t>(inc) - static_cast<uint32_t>(ex);
@@ -227,11 +276,12 @@ struct BucketStore {
         const uint64_t u0 = ex >> 32, u1 = inc >> 32;
         const uint32_t s = static_cast<uint32_t>(off[g] / n_sites);
         const uint64_t e0 = off[g] - s * n_sites, e1 = off[g + 1] - s * n_sites;  // list positions
+        const uint64_t C = chunk_of(e1 - e0, cc);
         const uint32_t ng = (c + kGroup - 1) / kGroup;
         uint64_t u = u0;
-        for (uint64_t blk = e0 / kChunk; blk * kChunk < e1 && u < u1; blk++) {
-            const uint64_t cb = blk * kChunk > e0 ? blk * kChunk : e0;
-            const uint64_t ce = (blk + 1) * kChunk < e1 ? (blk + 1) * kChunk : e1;
+        for (uint64_t blk = e0 / C; blk * C < e1 && u < u1; blk++) {
+            const uint64_t cb = blk * C > e0 ? blk * C : e0;
+            const uint64_t ce = (blk + 1) * C < e1 ? (blk + 1) * C : e1;
             const uint16_t len = static_cast<uint16_t>(ce - cb);
             for (uint32_t j = 0; j < ng; j++, u++) {
                 if (u >= unit_cap) return;
@@ -252,7 +302,7 @@ struct BucketStore {
 // entries are read once per group of up to kGroup guides)
 __global__ void k_bucket_stats(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off, uint64_t G,
                                const SliceGeom* __restrict__ geom, uint64_t n_sites, Counters* c) {
-    uint64_t buckets = 0, entries = 0, bytes = 0;
+    uint64_t buckets = 0, entries = 0, bytes = 0, cp[3] = {0, 0, 0};
     for (uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < G;
          g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint32_t k = cnt[g];
@@ -263,16 +313,20 @@ __global__ void k_bucket_stats(const uint32_t* __restrict__ cnt, const uint64_t*
         entries += (p1 - p0) * groups;
         // bit-sliced blocks copied: every block the bucket touches, once per guide group
         bytes += ((p1 - 1) / 32 - p0 / 32 + 1) * geom[s].wpb * 4ull * groups;
+        cp[(p1 - p0) < 64 ? 0 : (p1 - p0) < 4096 ? 1 : 2] += k;
     }
     for (int d = 16; d > 0; d >>= 1) {
         buckets += __shfl_down_sync(0xffffffffu, buckets, d);
         entries += __shfl_down_sync(0xffffffffu, entries, d);
         bytes += __shfl_down_sync(0xffffffffu, bytes, d);
+        for (int i = 0; i < 3; i++) cp[i] += __shfl_down_sync(0xffffffffu, cp[i], d);
     }
     if ((threadIdx.x & 31) == 0 && buckets) {
         atomicAdd(reinterpret_cast<unsigned long long*>(&c->buckets), buckets);
         atomicAdd(reinterpret_cast<unsigned long long*>(&c->entries), entries);
         atomicAdd(reinterpret_cast<unsigned long long*>(&c->rbytes), bytes);
+        for (int i = 0; i < 3; i++)
+            if (cp[i]) atomicAdd(reinterpret_cast<unsigned long long*>(&c->class_probes[i]), cp[i]);
     }
 }
 
@@ -283,13 +337,13 @@ __global__ void k_units_finalize(Counters* c, uint64_t unit_cap) {
 }
 
 // 3. guides grouped by bucket; each slot holds (guide index, guide residual code for the slice)
-__global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig, uint64_t n,
+__global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig, const uint32_t* d_n, uint64_t n,
                                 const uint32_t* __restrict__ probe_gb, uint32_t* __restrict__ bucket_cnt,
                                 const uint32_t* __restrict__ qstart, uint64_t* __restrict__ probe_qr) {
     __shared__ SliceGeom g[kMaxSlices];
     for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
     __syncthreads();
-    const uint64_t S = ix.n_slices, total = n * S;
+    const uint64_t S = ix.n_slices, total = guide_count(d_n, n) * S;
     for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < total;
          p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint32_t gb = probe_gb[p];
@@ -305,9 +359,9 @@ __global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig,
 // ---------------------------------------------------------------------------------------------
 // 4. the scan
 //
-// A unit is up to 32 bit-sliced blocks of 32 list positions (kChunk = 1024 entries) and up to
-// kGroup guides. Each warp runs its own kStages-deep ring in shared memory: for unit t + kStages
-// it issues two bulk copies (cp.async.bulk, the TMA engine) -- the unit's blocks and its guides'
+// A unit is up to 32 bit-sliced blocks of 32 list positions (at most kChunk = 1024 entries; the
+// unit size per bucket-size class is tunable) and up to kGroup guides. Each warp runs its own
+// ring of 2..4 stages in shared memory: for unit t + stages it issues two bulk copies (cp.async.bulk, the TMA engine) -- the unit's blocks and its guides'
 // (index, residual) pairs -- completing on the stage's mbarrier, while it computes unit t from
 // the stage that has landed. Lane l takes block l: per guide it forms the mismatch word of every
 // residual position (32 entries at once), adds them with a carry-save tree and keeps the entries
@@ -324,6 +378,7 @@ struct ScanArgs {
     uint32_t n_slices;
     uint32_t cand_cap;
     int max_dist;
+    const BatchHeader* hdr;  // batch form: the bound is the largest max_dist of the sets
     WarpLayout L;
 };
 
@@ -340,7 +395,7 @@ struct ScanCtx {  // per-warp state of the candidate slab
 // Compares every guide of the unit with the lane's block (RW residual positions per entry).
 template <int RW>
 __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb, const uint64_t* qr, uint32_t* qm,
-                                          const StageMeta& m, uint32_t wpb, int lane, ScanCtx& cx) {
+                                          const StageMeta& m, uint32_t wpb, int lane, int max_dist, ScanCtx& cx) {
     constexpr int NW = 2 * RW;
     constexpr int NV = (NW + 3) / 4;
     const unsigned lt = (1u << lane) - 1u;
@@ -374,7 +429,7 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
             if (2 * v < RW) mm[2 * v] = (d[4 * v] ^ w.x) | (d[4 * v + 1] ^ w.y);
             if (2 * v + 1 < RW) mm[2 * v + 1] = (d[4 * v + 2] ^ w.z) | (d[4 * v + 3] ^ w.w);
         }
-        uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), a.max_dist) & valid;
+        uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), max_dist) & valid;
         // candidates are rare: one per lane per round, written to the warp's slab as
         // (guide | slice << 26, list position, residual mismatch mask); k_cand_own applies the
         // ownership rule to the mask
@@ -405,13 +460,17 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
     }
 }
 
-// RWFIX > 0: every slice of the index has RWFIX residual positions; 0: mixed widths
+// RWFIX > 0: every slice of the index has RWFIX residual positions; 0: mixed widths.
+// Persistent and work-stealing: each warp takes batches of 32 consecutive units from a global
+// queue (one atomic per batch), so warps that draw heavy units (hot repeat buckets with a full
+// group of guides) simply take fewer batches.
 template <int RWFIX>
 __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     __shared__ ScanShared sh;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const WarpLayout L = a.L;
+    const uint32_t NS = L.stages;
     uint8_t* wbase_ptr = smem_raw + static_cast<size_t>(warp) * L.bytes;
     uint32_t* rb = reinterpret_cast<uint32_t*>(wbase_ptr);
     uint64_t* qr = reinterpret_cast<uint64_t*>(wbase_ptr + L.qr_off);
@@ -424,42 +483,51 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
         sh.rw[i] = a.geom[i].rwidth;
     }
     if (lane == 0) {
-        for (int st = 0; st < kStages; st++) mbar_init(&bar[st], 1);
+        for (uint32_t st = 0; st < NS; st++) mbar_init(&bar[st], 1);
         fence_barrier_init();
     }
     __syncthreads();
+    const int max_dist = a.hdr ? a.hdr->max_dist : a.max_dist;
 
     const uint32_t n_units = a.counters->n_units;
-    const uint32_t nwarps = gridDim.x * kScanWarps;
-    const uint32_t gw = blockIdx.x * kScanWarps + warp;
-    // this warp owns batches gw, gw + nwarps, ... of 32 consecutive units
     const uint32_t n_batches = (n_units + 31) / 32;
-    const uint32_t my_batches = n_batches > gw ? (n_batches - gw + nwarps - 1) / nwarps : 0;
-    uint32_t T = 0;
-    if (my_batches) {
-        const uint32_t last = gw + (my_batches - 1) * nwarps;
-        T = (my_batches - 1) * 32 + min(32u, n_units - last * 32);
-    }
-    auto load_desc = [&](uint32_t bi) -> uint4 {
-        const uint32_t u = (gw + bi * nwarps) * 32 + lane;
-        return (bi < my_batches && u < n_units) ? __ldg(reinterpret_cast<const uint4*>(a.units) + u)
-                                                : make_uint4(0, 0, 0, 0);
+    // descriptor of unit (batch b, slot lane); len 0 marks "no unit"
+    auto take_batch = [&]() -> uint4 {
+        uint32_t b = 0;
+        if (lane == 0) b = atomicAdd(&a.counters->next_batch, 1u);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        const uint32_t u = b * 32u + lane;
+        return (b < n_batches && u < n_units) ? __ldg(reinterpret_cast<const uint4*>(a.units) + u)
+                                              : make_uint4(0, 0, 0, 0);
     };
-    uint32_t ba = 0;
-    uint4 dA = load_desc(0), dB = load_desc(1);
+    uint4 dA = take_batch(), dB = make_uint4(0, 0, 0, 0);
+    bool have_b = false;
+    uint32_t issued = 0;  // units of this warp issued so far (unit t lives in ring stage t % NS)
+    uint32_t slot = 0;    // slot of the next unit in batch A
+    bool ended = false;
 
-    // issue the copies of unit t (all lanes call; lane 0 issues)
-    auto issue = [&](uint32_t t) {
-        if ((t >> 5) != ba) {
+    // issues the copies of the warp's next unit, if there is one (all lanes call; lane 0 issues)
+    auto try_issue = [&]() {
+        if (ended) return;
+        if (slot == 32) {
+            if (!have_b) dB = take_batch();
             dA = dB;
-            ba++;
-            dB = load_desc(ba + 1);
+            have_b = false;
+            slot = 0;
         }
-        const int src = t & 31;
-        const uint32_t p0 = __shfl_sync(0xffffffffu, dA.x, src), qbeg = __shfl_sync(0xffffffffu, dA.y, src);
-        const uint32_t dz = __shfl_sync(0xffffffffu, dA.z, src);
+        const uint32_t dz = __shfl_sync(0xffffffffu, dA.z, slot);
+        if ((dz & 0xFFFFu) == 0) {
+            ended = true;
+            return;
+        }
+        // take the following batch one unit early so its descriptor load overlaps this copy
+        if (slot == 31 && !have_b) {
+            dB = take_batch();
+            have_b = true;
+        }
+        const uint32_t p0 = __shfl_sync(0xffffffffu, dA.x, slot), qbeg = __shfl_sync(0xffffffffu, dA.y, slot);
         if (lane == 0) {
-            const int st = t % kStages;
+            const uint32_t st = issued % NS;
             const uint32_t len = dz & 0xFFFFu, qn = (dz >> 16) & 0xFFu, s = dz >> 24;
             const uint32_t b0 = p0 / 32u, nb = (p0 + len - 1) / 32u - b0 + 1;  // <= 32: inside one chunk
             const uint32_t wpb = sh.wpb[s];
@@ -484,18 +552,18 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
             bulk_copy_g2s(rb + st * L.stage_words, a.rbits + wa, rbytes, &bar[st]);
             bulk_copy_g2s(qr + st * kStageQr, a.probe_qr + qa0, qbytes, &bar[st]);
         }
+        slot++;
+        issued++;
     };
 
     ScanCtx cx{0u, 0u, false};
-    const uint32_t pro = T < kStages ? T : kStages;
-    for (uint32_t t = 0; t < pro; t++) issue(t);
+    for (uint32_t i = 0; i < NS; i++) try_issue();
     __syncwarp();
 
-    uint32_t t = 0;
+    uint32_t t = 0, st = 0, phase = 0;
     bool failed = false;
-    for (; t < T; t++) {
-        const int st = t % kStages;
-        const bool ok = mbar_wait_bounded(&bar[st], (t / kStages) & 1u, kWaitCycles);
+    for (; t < issued; t++) {
+        const bool ok = mbar_wait_bounded(&bar[st], phase, kWaitCycles);
         if (__any_sync(0xffffffffu, !ok)) {
             failed = true;
             break;
@@ -505,27 +573,30 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
         const uint32_t* srb = rb + st * L.stage_words;
         const uint64_t* sqr = qr + st * kStageQr;
         if constexpr (RWFIX > 0) {
-            scan_unit<RWFIX>(a, srb, sqr, qm, m, wpb, lane, cx);
+            scan_unit<RWFIX>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx);
         } else switch (sh.rw[m.s]) {  // uniform across the warp
-            case 12: scan_unit<12>(a, srb, sqr, qm, m, wpb, lane, cx); break;
-            case 10: scan_unit<10>(a, srb, sqr, qm, m, wpb, lane, cx); break;
-            case 16: scan_unit<16>(a, srb, sqr, qm, m, wpb, lane, cx); break;
-            case 15: scan_unit<15>(a, srb, sqr, qm, m, wpb, lane, cx); break;
-            case 14: scan_unit<14>(a, srb, sqr, qm, m, wpb, lane, cx); break;
-            case 13: scan_unit<13>(a, srb, sqr, qm, m, wpb, lane, cx); break;
-            case 11: scan_unit<11>(a, srb, sqr, qm, m, wpb, lane, cx); break;
-            case 9: scan_unit<9>(a, srb, sqr, qm, m, wpb, lane, cx); break;
-            case 8: scan_unit<8>(a, srb, sqr, qm, m, wpb, lane, cx); break;
-            default: scan_unit<7>(a, srb, sqr, qm, m, wpb, lane, cx); break;
+            case 12: scan_unit<12>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            case 10: scan_unit<10>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            case 16: scan_unit<16>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            case 15: scan_unit<15>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            case 14: scan_unit<14>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            case 13: scan_unit<13>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            case 11: scan_unit<11>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            case 9: scan_unit<9>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            case 8: scan_unit<8>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            default: scan_unit<7>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
         }
         __syncwarp();  // every lane is done with stage st before it is refilled
-        if (t + kStages < T) issue(t + kStages);
+        try_issue();
+        if (++st == NS) {
+            st = 0;
+            phase ^= 1u;
+        }
     }
     if (failed) {
         // a copy did not land in time: report, then wait (bounded) for this warp's copies in flight
         if (lane == 0) atomicOr(&a.counters->overflow, 4u);
-        for (uint32_t u = t; u < T && u < t + kStages; u++)
-            mbar_wait_bounded(&bar[u % kStages], (u / kStages) & 1u, kWaitCycles);
+        for (uint32_t u = t; u < issued; u++) mbar_wait_bounded(&bar[u % NS], (u / NS) & 1u, kWaitCycles);
     }
     for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
         if (i < a.cand_cap) a.cands[i] = make_uint4(kDeadCand, 0, 0, 0);
@@ -539,7 +610,8 @@ __global__ void k_cands_finalize(Counters* c, uint32_t cand_cap) {
 // earlier slice has all its positions matching, i.e. every earlier slice mask meets the
 // mismatch positions (the residual mismatch mask spread back to protospacer positions).
 // Rejected slots are marked dead; owned ones are counted per guide.
-__global__ void k_cand_own(uint4* __restrict__ cands, const Counters* c, IndexView ix, uint32_t* __restrict__ qhits) {
+__global__ void k_cand_own(uint4* __restrict__ cands, const Counters* c, IndexView ix, uint32_t* __restrict__ qhits,
+                           const SetDesc* __restrict__ sets, const uint16_t* __restrict__ qset) {
     __shared__ uint32_t s_pmask[kMaxSlices];
     __shared__ uint8_t s_rpos[kMaxSlices][kSeqLen];
     for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) {
@@ -553,6 +625,13 @@ __global__ void k_cand_own(uint4* __restrict__ cands, const Counters* c, IndexVi
         const uint4 r = cands[i];
         if (r.x == kDeadCand) continue;
         const uint32_t s = r.x >> kGuideBits;
+        const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
+        // batch form: the scan kept candidates up to the largest bound of the batch's sets; the
+        // residual mismatch count is the site's distance (the slice positions all match)
+        if (qset && __popc(r.z) > sets[qset[q]].P.max_dist) {
+            cands[i].x = kDeadCand;
+            continue;
+        }
         uint32_t mism20 = 0, mm = r.z;
         while (mm) {
             mism20 |= 1u << s_rpos[s][__ffs(mm) - 1];
@@ -565,7 +644,7 @@ __global__ void k_cand_own(uint4* __restrict__ cands, const Counters* c, IndexVi
                 break;
             }
         if (own)
-            atomicAdd(&qhits[r.x & ((1u << kGuideBits) - 1u)], 1u);
+            atomicAdd(&qhits[q], 1u);
         else
             cands[i].x = kDeadCand;
     }
@@ -577,9 +656,14 @@ struct LoadQhits {
     const uint32_t* p;
     __device__ uint32_t operator()(uint64_t i) const { return p[i]; }
 };
+// p[n] receives the total: element i also writes its inclusive prefix to p[i + 1] (the same
+// value element i + 1 writes as its exclusive prefix)
 struct StoreQoff {
     uint32_t* p;
-    __device__ void operator()(uint64_t i, uint32_t ex, uint32_t) const { p[i] = ex; }
+    __device__ void operator()(uint64_t i, uint32_t ex, uint32_t inc) const {
+        p[i] = ex;
+        p[i + 1] = inc;
+    }
 };
 
 // One thread per owned hit (many independent loads in flight): the site id, then the site record
@@ -713,12 +797,19 @@ struct ScoreArgs {
     uint32_t* exitq;
     uint32_t* bitmap;
     uint64_t n;
-    ScoreParams P;
+    const uint32_t* d_n;     // batch form: guide count on the device
+    ScoreParams P;           // plain form: one parameter set for every guide
+    const SetDesc* sets;     // batch form: per-set parameters, guide qi belongs to set qset[qi]
+    const uint16_t* qset;
     double* out_mit;
     double* out_cfd;
     char* out_code;
     uint64_t* out_count;
 };
+
+__device__ __forceinline__ ScoreParams params_of(const ScoreArgs& a, uint64_t qi) {
+    return a.qset ? a.sets[a.qset[qi]].P : a.P;
+}
 
 // Exact sums. Every contribution (MIT value x occurrences, CFD product x occurrences) lies in
 // [6e-6, 2^33) and has no bit below 2^-84, so it converts exactly to a 128-bit fixed point
@@ -768,9 +859,9 @@ struct FxContribution {
 };
 
 // r: seg record (position, slice, site id, occurrences), sig: the site's signature
-__device__ __forceinline__ FxContribution fx_contribution(const ScoreArgs& a, const Tables& T, uint64_t q, const uint4& r,
-                                                         uint64_t sig) {
-    const Contribution c = contribution(T, a.P, q, sig, r.w);
+__device__ __forceinline__ FxContribution fx_contribution(const ScoreParams& P, const Tables& T, uint64_t q,
+                                                         const uint4& r, uint64_t sig) {
+    const Contribution c = contribution(T, P, q, sig, r.w);
     return FxContribution{fx_from(c.mit), fx_from(c.cfd), c.occ};
 }
 
@@ -785,7 +876,9 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
     const Tables& T = *a.tables;
     if (a.counters->overflow) return;  // rerun follows
     const uint64_t gw = blockIdx.x * 8ull + warp, nw = gridDim.x * 8ull;
-    for (uint64_t qi = gw; qi < a.n; qi += nw) {
+    const uint64_t n = guide_count(a.d_n, a.n);
+    for (uint64_t qi = gw; qi < n; qi += nw) {
+        const ScoreParams P = params_of(a, qi);
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         const uint64_t q = a.qsig[qi];
         const uint4* seg = a.seg + h0;
@@ -793,7 +886,7 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         Fx tm{0, 0}, tc{0, 0};
         uint64_t tn = 0;
         for (uint32_t i = lane; i < L; i += 32) {
-            const FxContribution c = fx_contribution(a, T, q, seg[i], sig[i]);
+            const FxContribution c = fx_contribution(P, T, q, seg[i], sig[i]);
             tm = fx_add(tm, c.mit);
             tc = fx_add(tc, c.cfd);
             tn += c.occ;
@@ -801,7 +894,7 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         tm = fx_warp_sum(tm);
         tc = fx_warp_sum(tc);
         for (int d = 16; d > 0; d >>= 1) tn += __shfl_xor_sync(0xffffffffu, tn, d);
-        if (exit_test(a.P, fx_double(tm), fx_double(tc))) {
+        if (exit_test(P, fx_double(tm), fx_double(tc))) {
             if (lane == 0) {
                 if (L <= static_cast<uint32_t>(kWarpSort))
                     a.exitq[atomicAdd(&a.counters->n_exit, 1u)] = static_cast<uint32_t>(qi);
@@ -810,13 +903,13 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
             }
             continue;
         }
-        if (a.P.want_distinct)
+        if (P.want_distinct)
             for (uint32_t i = lane; i < L; i += 32) {
                 const uint32_t id = seg[i].z;
                 atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
         if (lane == 0)
-            finalise(a.P, fx_double(tm), fx_double(tc), tn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+            finalise(P, fx_double(tm), fx_double(tc), tn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
     }
 }
 
@@ -844,6 +937,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
     const uint32_t gw = blockIdx.x * 8 + warp, nw = gridDim.x * 8;
     for (uint32_t e = gw; e < n_exit; e += nw) {
         const uint64_t qi = a.exitq[e];
+        const ScoreParams P = params_of(a, qi);
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         const uint64_t q = a.qsig[qi];
         const uint4* seg = a.seg + h0;
@@ -876,7 +970,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             uint64_t tn = 0;
             for (uint32_t j = lane; j < ns; j += 32) {
                 const uint32_t h = W.idx[b0 + j];
-                const FxContribution c = fx_contribution(a, T, q, seg[h], sig[h]);
+                const FxContribution c = fx_contribution(P, T, q, seg[h], sig[h]);
                 tm = fx_add(tm, c.mit);
                 tc = fx_add(tc, c.cfd);
                 tn += c.occ;
@@ -884,8 +978,8 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             tm = fx_add(fx_warp_sum(tm), rm);
             tc = fx_add(fx_warp_sum(tc), rc);
             for (int d = 16; d > 0; d >>= 1) tn += __shfl_xor_sync(0xffffffffu, tn, d);
-            if (!exit_test(a.P, fx_double(tm), fx_double(tc))) {
-                if (a.P.want_distinct)
+            if (!exit_test(P, fx_double(tm), fx_double(tc))) {
+                if (P.want_distinct)
                     for (uint32_t j = lane; j < ns; j += 32) {
                         const uint32_t id = seg[W.idx[b0 + j]].z;
                         atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
@@ -925,15 +1019,15 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
                     const uint32_t h = W.keys[t] & 1023u;
                     const uint4 r = seg[h];
                     id = r.z;
-                    c = fx_contribution(a, T, q, r, sig[h]);
+                    c = fx_contribution(P, T, q, r, sig[h]);
                 }
                 const Fx im = fx_add(fx_warp_incl(c.mit, lane), rm);
                 const Fx ic = fx_add(fx_warp_incl(c.cfd, lane), rc);
                 const uint64_t in = warp_incl_sum_u64(c.occ, lane) + rn;
-                const bool ex = t < ns && exit_test(a.P, fx_double(im), fx_double(ic));
+                const bool ex = t < ns && exit_test(P, fx_double(im), fx_double(ic));
                 const unsigned em = __ballot_sync(0xffffffffu, ex);
                 const int last = em ? __ffs(em) - 1 : (ns - c0 >= 32 ? 31 : static_cast<int>(ns - c0 - 1));
-                if (a.P.want_distinct && t < ns && lane <= last) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                if (P.want_distinct && t < ns && lane <= last) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
                 rm = Fx{__shfl_sync(0xffffffffu, im.hi, last), __shfl_sync(0xffffffffu, im.lo, last)};
                 rc = Fx{__shfl_sync(0xffffffffu, ic.hi, last), __shfl_sync(0xffffffffu, ic.lo, last)};
                 rn = __shfl_sync(0xffffffffu, in, last);
@@ -941,7 +1035,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             }
             __syncwarp();
         }
-        if (lane == 0) finalise(a.P, fx_double(rm), fx_double(rc), rn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+        if (lane == 0) finalise(P, fx_double(rm), fx_double(rc), rn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
         __syncwarp();
     }
 }
@@ -963,6 +1057,7 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
     const uint32_t n_big = a.counters->n_big;
     for (uint32_t b = blockIdx.x; b < n_big; b += gridDim.x) {
         const uint64_t qi = a.big[b];
+        const ScoreParams P = params_of(a, qi);
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         uint4* seg = a.seg + h0;
         uint64_t* sig = a.segsig + h0;
@@ -1011,7 +1106,7 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
                 const uint32_t h = in_smem ? static_cast<uint32_t>(s_bkeys[t] & ((1u << kBlockIdxBits) - 1)) : t;
                 const uint4 r = seg[h];
                 id = r.z;
-                c = fx_contribution(a, T, q, r, sig[h]);
+                c = fx_contribution(P, T, q, r, sig[h]);
             }
             Fx im = fx_warp_incl(c.mit, lane), ic = fx_warp_incl(c.cfd, lane);
             uint64_t in = warp_incl_sum_u64(c.occ, lane);
@@ -1032,12 +1127,12 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             im = fx_add(im, pm);
             ic = fx_add(ic, pc);
             in += pn;
-            if (t < L && exit_test(a.P, fx_double(im), fx_double(ic))) atomicMin(&s_first, static_cast<int>(threadIdx.x));
+            if (t < L && exit_test(P, fx_double(im), fx_double(ic))) atomicMin(&s_first, static_cast<int>(threadIdx.x));
             __syncthreads();
             const int first = s_first;
             const uint32_t in_chunk = L - c0 < blockDim.x ? L - c0 : blockDim.x;
             const int last = first != 0x7fffffff ? first : static_cast<int>(in_chunk) - 1;
-            if (a.P.want_distinct && t < L && static_cast<int>(threadIdx.x) <= last)
+            if (P.want_distinct && t < L && static_cast<int>(threadIdx.x) <= last)
                 atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             __syncthreads();
             if (static_cast<int>(threadIdx.x) == last) {
@@ -1053,7 +1148,7 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             __syncthreads();
         }
         if (threadIdx.x == 0)
-            finalise(a.P, fx_double(run_m), fx_double(run_c), run_n, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+            finalise(P, fx_double(run_m), fx_double(run_c), run_n, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
         __syncthreads();
     }
 }
@@ -1103,46 +1198,69 @@ void init_tables(Workspace& ws, cudaStream_t st) {
     ISSL_CUDA(cudaStreamSynchronize(st));
 }
 
+uint32_t max_wpb_of(const issl_index* ix) {
+    uint32_t m = 4;
+    for (auto& g : ix->geom) m = std::max<uint32_t>(m, g.wpb);
+    return m;
+}
+
+// A workspace holds every per-call buffer of the pipeline. The index keeps one for the plain
+// entry points; batch contexts and server slots own theirs, so calls on different workspaces
+// can run concurrently against the same resident index.
+std::unique_ptr<Workspace> new_workspace(issl_index* ix) {
+    auto ws = std::make_unique<Workspace>();
+    ws->device = ix->device;
+    ISSL_CUDA(cudaStreamCreateWithFlags(&ws->own_stream, cudaStreamNonBlocking));
+    ISSL_CUDA(cudaStreamCreateWithFlags(&ws->cap_stream, cudaStreamNonBlocking));
+    for (auto& e : ws->ev) ISSL_CUDA(cudaEventCreate(&e));
+    // one residual width for every slice (the usual case) selects a specialised scan
+    ws->scan_rw = ix->geom.empty() ? 0 : ix->geom[0].rwidth;
+    for (auto& g : ix->geom)
+        if (g.rwidth != ws->scan_rw) ws->scan_rw = 0;
+    if (ws->scan_rw != 12 && ws->scan_rw != 10 && ws->scan_rw != 16) ws->scan_rw = 0;
+    const int smem_max = static_cast<int>(kScanWarps * warp_layout(max_wpb_of(ix), kMaxStages).bytes);
+    ISSL_CUDA(cudaFuncSetAttribute(scan_kernel(ws->scan_rw), cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+    ISSL_CUDA(cudaFuncSetAttribute(k_score_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kBlockHits * sizeof(uint64_t))));
+    ISSL_CUDA(cudaFuncSetAttribute(k_score_ordered, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(8 * sizeof(OrderedSmem))));
+    ws->counters.reserve(1);
+    ws->scan64.reserve(kScanBlocks + 4);
+    ws->scan32.reserve(kScanBlocks + 4);
+    init_tables(*ws, ws->own_stream);
+    return ws;
+}
+
 Workspace& workspace(issl_index* ix) {
-    if (!ix->ws) {
-        auto ws = std::make_unique<Workspace>();
-        ws->device = ix->device;
-        ISSL_CUDA(cudaStreamCreateWithFlags(&ws->own_stream, cudaStreamNonBlocking));
-        for (auto& e : ws->ev) ISSL_CUDA(cudaEventCreate(&e));
-        int per_sm = 0;
-        uint32_t max_wpb = 4;
-        for (auto& g : ix->geom) max_wpb = std::max<uint32_t>(max_wpb, g.wpb);
-        ws->scan_layout = warp_layout(max_wpb);
-        ws->scan_smem = static_cast<int>(kScanWarps * ws->scan_layout.bytes);
-        // one residual width for every slice (the usual case) selects a specialised scan
-        ws->scan_rw = ix->geom.empty() ? 0 : ix->geom[0].rwidth;
-        for (auto& g : ix->geom)
-            if (g.rwidth != ws->scan_rw) ws->scan_rw = 0;
-        if (ws->scan_rw != 12 && ws->scan_rw != 10 && ws->scan_rw != 16) ws->scan_rw = 0;
-        const void* kfn = scan_kernel(ws->scan_rw);
-        ISSL_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, ws->scan_smem));
-        ISSL_CUDA(cudaFuncSetAttribute(k_score_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(kBlockHits * sizeof(uint64_t))));
-        ISSL_CUDA(cudaFuncSetAttribute(k_score_ordered, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(8 * sizeof(OrderedSmem))));
-        ISSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kScanWarps * 32, ws->scan_smem));
-        ws->scan_blocks = sm_count(ix->device) * std::max(per_sm, 1);
-        ws->counters.reserve(1);
-        ws->scan64.reserve(kScanBlocks + 4);
-        ws->scan32.reserve(kScanBlocks + 4);
-        init_tables(*ws, ws->own_stream);
-        ix->ws = std::move(ws);
-    }
+    if (!ix->ws) ix->ws = new_workspace(ix);
     return *ix->ws;
 }
 
-void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, cudaStream_t st) {
+// Configures the scan for the index's current tuning (staging depth -> shared memory layout,
+// blocks per SM -> persistent grid).
+void apply_tuning(issl_index* ix, Workspace& ws) {
+    if (ws.tuning_version == ix->tuning_version) return;
+    const issl_tuning& t = ix->tuning;
+    ws.scan_layout = warp_layout(max_wpb_of(ix), t.stages);
+    ws.scan_smem = static_cast<int>(kScanWarps * ws.scan_layout.bytes);
+    int per_sm = 0;
+    ISSL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_kernel(ws.scan_rw), kScanWarps * 32,
+                                                            ws.scan_smem));
+    per_sm = std::max(per_sm, 1);
+    if (t.blocks_per_sm) per_sm = std::min<int>(per_sm, static_cast<int>(t.blocks_per_sm));
+    ws.scan_blocks = sm_count(ix->device) * per_sm;
+    ws.tuning_version = ix->tuning_version;
+}
+
+void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st) {
     const uint64_t S = ix->n_slices, G = ix->n_buckets;
+    apply_tuning(ix, ws);
     if (ws.g_cap < G + 1) {
         ws.bucket_cnt.reserve(G + 1);
         ws.bucket_qstart.reserve(G + 1);
         ISSL_CUDA(cudaMemsetAsync(ws.bucket_cnt.p, 0, (G + 1) * 4, st));
         ws.g_cap = G + 1;
+        ws.epoch++;
     }
     if (ws.q_cap < n || !ws.qhits.p) {
         const size_t cap = std::max<size_t>(n, 1024);
@@ -1158,19 +1276,29 @@ void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, cudaStream_t st) {
         ws.out_code.reserve(cap);
         ws.out_count.reserve(cap);
         ws.out_distinct.reserve(1);
+        if (ws.qset.p) ws.qset.reserve(cap);
         ISSL_CUDA(cudaMemsetAsync(ws.qhits.p, 0, (cap + 1) * 4, st));
         ws.q_cap = cap;
+        ws.epoch++;
+    }
+    if (batch && !ws.qset.p) {
+        ws.qset.reserve(ws.q_cap);
+        ws.epoch++;
     }
     if (!ws.zero_state_ok) {
         ISSL_CUDA(cudaMemsetAsync(ws.bucket_cnt.p, 0, (G + 1) * 4, st));
         ISSL_CUDA(cudaMemsetAsync(ws.qhits.p, 0, (ws.q_cap + 1) * 4, st));
         ws.zero_state_ok = true;
     }
-    // first guesses: ~2.5 units per probe plus headroom; hits grow on demand
-    const size_t want_units = std::max<size_t>(ws.unit_cap, n * S * 3 + 4096);
+    // first guesses: ~2.5 units per probe with 1024-entry units (more with smaller ones) plus
+    // headroom; hits grow on demand
+    uint32_t min_chunk = kChunk;
+    for (uint32_t c : ix->tuning.chunk) min_chunk = std::min(min_chunk, c);
+    const size_t want_units = std::max<size_t>(ws.unit_cap, n * S * 3 * (kChunk / min_chunk) + 4096);
     if (ws.unit_cap < want_units) {
         ws.units.reserve(want_units);
         ws.unit_cap = want_units;
+        ws.epoch++;
     }
     // candidates: a first guess plus one slab of slack per scan warp; grown on demand
     const size_t want_cands = std::max<size_t>(
@@ -1180,8 +1308,27 @@ void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, cudaStream_t st) {
         ws.seg.reserve(want_cands);
         ws.segsig.reserve(want_cands);
         ws.cand_cap = want_cands;
+        ws.epoch++;
     }
 }
+
+}  // namespace
+
+// The allocations of ensure_capacity as a formula: a fixed part, bytes per guide and bytes per
+// candidate slot (candidate record, grouped hit record, grouped hit signature).
+void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide, uint64_t* per_candidate) {
+    const uint64_t S = ix->n_slices, G = ix->n_buckets;
+    uint32_t min_chunk = kChunk;
+    for (uint32_t c : ix->tuning.chunk) min_chunk = std::min(min_chunk, c);
+    const uint64_t slab_slack = 148ull * 16 * kScanWarps * kCandSlab;  // one slab per scan warp, at most
+    *per_candidate = sizeof(uint4) * 2 + sizeof(uint64_t);
+    *fixed = 8 * (G + 1) + sizeof(Tables) + sizeof(Counters) + (kScanBlocks + 4) * 12 + 4096 * sizeof(UnitDesc) +
+             (65536 + slab_slack) * *per_candidate;
+    // qsig, probe lists, hit counts and offsets, exit queues, outputs, set map; scan units
+    *per_guide = 8 + 12 * S + 4 * 4 + (8 + 8 + 1 + 8) + 2 + sizeof(UnitDesc) * 3 * S * (kChunk / min_chunk);
+}
+
+namespace {
 
 ScoreParams make_params(int method, double threshold, int max_dist, bool want_distinct) {
     ISSL_REQUIRE(method >= ISSL_METHOD_MIT && method <= ISSL_METHOD_AVG_MIT_CFD, ISSL_ERR_ARG,
@@ -1196,6 +1343,7 @@ ScoreParams make_params(int method, double threshold, int max_dist, bool want_di
     P.threshold = threshold;
     P.maximum_sum = (10000.0 - threshold * 100) / threshold;
     P.want_distinct = want_distinct ? 1 : 0;
+    P.pad = 0;
     return P;
 }
 
@@ -1206,24 +1354,66 @@ inline unsigned grid_for(uint64_t n, unsigned threads, unsigned cap) {
     return static_cast<unsigned>(b);
 }
 
-// Enqueues the whole pipeline for n guides whose signatures are in ws.qsig (or d_qsig).
-void enqueue_pipeline(issl_index* ix, Workspace& ws, const uint64_t* d_qsig, uint64_t n, const ScoreParams& P,
-                      double* d_mit, double* d_cfd, char* d_code, uint64_t* d_count, cudaStream_t st) {
+// One pipeline run. Plain form: n guides, one parameter set P, sizes known on the host.
+// Batch form: up to n (the capacity) guides, the count and the set table read on the device
+// from `hdr` / `sets`, so that the enqueued work can be captured once and replayed.
+struct RunSpec {
+    const uint64_t* qsig = nullptr;
+    uint64_t n = 0;
+    ScoreParams P{};
+    const BatchHeader* hdr = nullptr;
+    const SetDesc* sets = nullptr;
+    double* mit = nullptr;
+    double* cfd = nullptr;
+    char* code = nullptr;
+    uint64_t* count = nullptr;
+    bool events = true;  // record the timing events (not inside a graph capture)
+};
+
+__global__ void k_expand_sets(const BatchHeader* __restrict__ hdr, const SetDesc* __restrict__ sets,
+                              uint16_t* __restrict__ qset) {
+    const uint32_t n = hdr->n, ns = hdr->n_sets;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = ns - 1;  // last set whose begin <= i
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (sets[mid].begin <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        qset[i] = static_cast<uint16_t>(lo);
+    }
+}
+
+// Enqueues the whole pipeline. Returns the number of kernels it launched.
+uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaStream_t st) {
     const IndexView v = ix->view();
-    const uint64_t S = ix->n_slices, G = ix->n_buckets;
+    const uint64_t S = ix->n_slices, G = ix->n_buckets, n = R.n;
+    const bool batch = R.hdr != nullptr;
+    const uint32_t* d_n = batch ? &R.hdr->n : nullptr;
+    const uint16_t* qset = batch ? ws.qset.p : nullptr;
     const int sms = sm_count(ix->device);
+    const issl_tuning& tn = ix->tuning;
+    const ChunkClasses cc{{tn.chunk[0], tn.chunk[1], tn.chunk[2]}};
+    uint64_t k = 0;
     ISSL_CUDA(cudaMemsetAsync(ws.counters.p, 0, sizeof(Counters), st));
     const uint64_t* off = ix->offsets.p;
-    ISSL_CUDA(cudaEventRecord(ws.ev[0], st));
-    k_probe_count<<<grid_for(n * S, 256, sms * 16), 256, 0, st>>>(v, d_qsig, n, ws.probe_gb.p, ws.bucket_cnt.p, off);
-    device_scan<uint64_t, OpSum>(BucketLoad{ws.bucket_cnt.p, off, ix->n_sites},
+    if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[0], st));
+    if (batch) {
+        k_expand_sets<<<grid_for(n, 256, sms * 8), 256, 0, st>>>(R.hdr, R.sets, ws.qset.p);
+        k++;
+    }
+    k_probe_count<<<grid_for(n * S, 256, sms * 16), 256, 0, st>>>(v, R.qsig, d_n, n, ws.probe_gb.p, ws.bucket_cnt.p,
+                                                                   off);
+    device_scan<uint64_t, OpSum>(BucketLoad{ws.bucket_cnt.p, off, ix->n_sites, cc},
                                  BucketStore{ws.bucket_cnt.p, off, ws.bucket_qstart.p, ws.units.p, ws.unit_cap,
-                                             ix->n_sites},
+                                             ix->n_sites, cc},
                                  nullptr, G, ws.scan64.p, &ws.counters.p->bucket_total, st);
     k_units_finalize<<<1, 1, 0, st>>>(ws.counters.p, ws.unit_cap);
     k_bucket_stats<<<sms * 4, 256, 0, st>>>(ws.bucket_cnt.p, off, G, ix->d_geom.p, ix->n_sites, ws.counters.p);
-    k_probe_scatter<<<grid_for(n * S, 256, sms * 16), 256, 0, st>>>(v, d_qsig, n, ws.probe_gb.p, ws.bucket_cnt.p,
-                                                                     ws.bucket_qstart.p, ws.probe_qr.p);
+    k_probe_scatter<<<grid_for(n * S, 256, sms * 16), 256, 0, st>>>(v, R.qsig, d_n, n, ws.probe_gb.p,
+                                                                     ws.bucket_cnt.p, ws.bucket_qstart.p,
+                                                                     ws.probe_qr.p);
+    k += 7;
     ScanArgs sa;
     sa.rbits = ix->rbits.p;
     sa.geom = ix->d_geom.p;
@@ -1233,26 +1423,28 @@ void enqueue_pipeline(issl_index* ix, Workspace& ws, const uint64_t* d_qsig, uin
     sa.cands = ws.cands.p;
     sa.n_slices = static_cast<uint32_t>(S);
     sa.cand_cap = static_cast<uint32_t>(std::min<size_t>(ws.cand_cap, 0xFFFFFFFFull));
-    sa.max_dist = P.max_dist;
+    sa.max_dist = R.P.max_dist;
+    sa.hdr = R.hdr;
     sa.L = ws.scan_layout;
-    ISSL_CUDA(cudaEventRecord(ws.ev[1], st));
+    if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[1], st));
     switch (ws.scan_rw) {
         case 12: k_scan<12><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
         case 10: k_scan<10><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
         case 16: k_scan<16><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
         default: k_scan<0><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
     }
-    ISSL_CUDA(cudaEventRecord(ws.ev[2], st));
+    if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[2], st));
     k_cands_finalize<<<1, 1, 0, st>>>(ws.counters.p, sa.cand_cap);
-    k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, v, ws.qhits.p);
-    device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, nullptr, n, ws.scan32.p,
-                                 ws.qhoff.p + n, st);
+    k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, v, ws.qhits.p, R.sets, qset);
+    device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, d_n, n, ws.scan32.p,
+                                 &ws.counters.p->hit_total, st);
     k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, ws.qhits.p, ws.qhoff.p, v, ws.seg.p,
                                            ws.segsig.p);
-    if (P.want_distinct) ISSL_CUDA(cudaMemsetAsync(ws.bitmap.p, 0, (ix->n_sites / 32 + 1) * 4, st));
+    k += 7;
+    if (R.P.want_distinct) ISSL_CUDA(cudaMemsetAsync(ws.bitmap.p, 0, (ix->n_sites / 32 + 1) * 4, st));
     ScoreArgs a;
     a.ix = v;
-    a.qsig = d_qsig;
+    a.qsig = R.qsig;
     a.seg = ws.seg.p;
     a.segsig = ws.segsig.p;
     a.exitq = ws.exitq.p;
@@ -1262,28 +1454,31 @@ void enqueue_pipeline(issl_index* ix, Workspace& ws, const uint64_t* d_qsig, uin
     a.big = ws.big.p;
     a.bitmap = ws.bitmap.p;
     a.n = n;
-    a.P = P;
-    a.out_mit = d_mit;
-    a.out_cfd = d_cfd;
-    a.out_code = d_code;
-    a.out_count = d_count;
+    a.d_n = d_n;
+    a.P = R.P;
+    a.sets = R.sets;
+    a.qset = qset;
+    a.out_mit = R.mit;
+    a.out_cfd = R.cfd;
+    a.out_code = R.code;
+    a.out_count = R.count;
     k_score_sum<<<grid_for(n, 8, sms * 8), 256, 0, st>>>(a);
     k_score_ordered<<<sms * 4, 256, 8 * sizeof(OrderedSmem), st>>>(a);
     k_score_block<<<sms * 2, 256, kBlockHits * sizeof(uint64_t), st>>>(a);
-    if (P.want_distinct) k_popcount<<<sms * 4, 256, 0, st>>>(ws.bitmap.p, ix->n_sites / 32 + 1, ws.counters.p);
-    ISSL_CUDA(cudaEventRecord(ws.ev[3], st));
+    k += 3;
+    if (R.P.want_distinct) {
+        k_popcount<<<sms * 4, 256, 0, st>>>(ws.bitmap.p, ix->n_sites / 32 + 1, ws.counters.p);
+        k++;
+    }
+    if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[3], st));
     ISSL_CUDA(cudaGetLastError());
-    // probe_count, 3 bucket-scan, units_finalize, bucket_stats, probe_scatter, scan,
-    // cands_finalize, cand_own, 3 hit-offset scan, hit_scatter, score_sum, score_ordered,
-    // score_block (+ popcount for distinct counts)
-    ws.launches += 17 + (P.want_distinct ? 1 : 0);
+    return k;
 }
 
 // Reads the counters after a pipeline run; returns false (and grows capacities) on overflow.
-bool check_and_grow(issl_index* ix, Workspace& ws, uint64_t n, cudaStream_t st) {
+bool check_and_grow(Workspace& ws, cudaStream_t st) {
     Counters c;
     ISSL_CUDA(cudaMemcpyAsync(&c, ws.counters.p, sizeof c, cudaMemcpyDeviceToHost, st));
-    ISSL_CUDA(cudaMemcpyAsync(&c.hit_total, ws.qhoff.p + n, 4, cudaMemcpyDeviceToHost, st));
     ISSL_CUDA(cudaStreamSynchronize(st));
     ws.last = c;
     if (c.overflow & 4u) {
@@ -1307,17 +1502,16 @@ bool check_and_grow(issl_index* ix, Workspace& ws, uint64_t n, cudaStream_t st) 
         ws.cand_cap = cap;
         ok = false;
     }
-    if (!ok) ws.zero_state_ok = false;  // counters of the aborted run are not drained
+    if (!ok) {
+        ws.zero_state_ok = false;  // counters of the aborted run are not drained
+        ws.epoch++;
+    }
     return ok;
 }
 
-void record_stats(issl_index* ix, Workspace& ws, uint64_t n) {
-    float scan = 0.f, total = 0.f;
-    cudaEventElapsedTime(&scan, ws.ev[1], ws.ev[2]);
-    cudaEventElapsedTime(&total, ws.ev[0], ws.ev[3]);
-    issl_score_stats& s = ix->stats;
-    s.scan_ms = scan;
-    s.total_ms = total;
+void fill_stats(const Workspace& ws, float scan_ms, float total_ms, uint64_t launches, issl_score_stats& s) {
+    s.scan_ms = scan_ms;
+    s.total_ms = total_ms;
     s.probes = static_cast<uint64_t>(ws.last.bucket_total & 0xFFFFFFFFull);
     s.units = ws.last.bucket_total >> 32;
     s.hits = ws.last.hit_total;
@@ -1326,32 +1520,159 @@ void record_stats(issl_index* ix, Workspace& ws, uint64_t n) {
     // bytes the scan must move: the bit-sliced blocks it copies, 16 per unit descriptor, 8 per
     // guide of a unit (index + residual), 16 per candidate slot written
     s.scan_bytes = ws.last.rbytes + 16 * s.units + 8 * s.probes + 16 * static_cast<uint64_t>(ws.last.n_cand);
-    s.launches = ws.launches;
+    s.launches = launches;
+    for (int i = 0; i < 3; i++) s.class_probes[i] = ws.last.class_probes[i];
+    s.candidates = ws.last.n_cand;
+}
+
+void record_stats(issl_index* ix, Workspace& ws) {
+    float scan = 0.f, total = 0.f;
+    cudaEventElapsedTime(&scan, ws.ev[1], ws.ev[2]);
+    cudaEventElapsedTime(&total, ws.ev[0], ws.ev[3]);
+    fill_stats(ws, scan, total, ws.launches, ix->stats);
     ws.launches = 0;
-    (void)n;
 }
 
 void run_scoring(issl_index* ix, const uint64_t* d_qsig_in, uint64_t n, const ScoreParams& P, double* d_mit,
-                 double* d_cfd, char* d_code, uint64_t* d_count, uint64_t* d_distinct, cudaStream_t st,
-                 bool sync_and_check) {
+                 double* d_cfd, char* d_code, uint64_t* d_count, uint64_t* d_distinct, cudaStream_t st) {
     Workspace& ws = workspace(ix);
     if (P.want_distinct) ws.bitmap.reserve(ix->n_sites / 32 + 1);
+    RunSpec R;
+    R.qsig = d_qsig_in;
+    R.n = n;
+    R.P = P;
+    R.mit = d_mit;
+    R.cfd = d_cfd;
+    R.code = d_code;
+    R.count = d_count;
     for (int attempt = 0; attempt < 4; attempt++) {
-        ensure_capacity(ix, ws, n, st);
-        enqueue_pipeline(ix, ws, d_qsig_in, n, P, d_mit, d_cfd, d_code, d_count, st);
+        ensure_capacity(ix, ws, n, false, st);
+        ws.launches += enqueue_pipeline(ix, ws, R, st);
         if (d_distinct) {
             k_copy_distinct<<<1, 1, 0, st>>>(ws.counters.p, d_distinct);
             ws.launches++;
         }
-        if (!sync_and_check) {
-            // device-buffer path: one check per call keeps the workspace honest
-        }
-        if (check_and_grow(ix, ws, n, st)) {
-            record_stats(ix, ws, n);
+        if (check_and_grow(ws, st)) {
+            record_stats(ix, ws);
             return;
         }
     }
     throw Error(ISSL_ERR_NOMEM, "scoring workspace kept overflowing");
+}
+
+}  // namespace
+}  // namespace issl
+
+// ---------------------------------------------------------------------------------------------
+// batch contexts
+struct issl_batch {
+    issl_index* ix = nullptr;
+    std::unique_ptr<issl::Workspace> ws;
+    issl_score_stats stats{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~issl_batch() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+namespace issl {
+namespace {
+
+constexpr size_t kMaxSets = 65535;
+
+// Scores ws.qsig[0..n) split into the given sets; results land in ws.out_*.
+void run_batch(issl_batch* b, uint64_t n, const issl_guide_set* sets, size_t n_sets, cudaStream_t st) {
+    issl_index* ix = b->ix;
+    Workspace& ws = *b->ws;
+    // the set table, staged in pinned memory so that its upload is an ordinary async copy
+    const size_t table_bytes = sizeof(BatchHeader) + n_sets * sizeof(SetDesc);
+    if (ws.sets_cap < n_sets) {
+        const size_t cap = std::max<size_t>(n_sets, 256);
+        ISSL_CUDA(cudaStreamSynchronize(st));
+        if (ws.h_batch) cudaFreeHost(ws.h_batch);
+        ws.h_batch = nullptr;
+        ISSL_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ws.h_batch), sizeof(BatchHeader) + cap * sizeof(SetDesc),
+                                cudaHostAllocDefault));
+        ws.batch.reserve(sizeof(BatchHeader) + cap * sizeof(SetDesc));
+        ws.sets_cap = cap;
+        ws.epoch++;
+    }
+    BatchHeader h{};
+    h.n = static_cast<uint32_t>(n);
+    h.n_sets = static_cast<uint32_t>(n_sets);
+    h.max_dist = 0;
+    SetDesc* hs = reinterpret_cast<SetDesc*>(ws.h_batch + sizeof(BatchHeader));
+    uint64_t begin = 0;
+    for (size_t i = 0; i < n_sets; i++) {
+        hs[i].P = make_params(sets[i].method, sets[i].threshold, sets[i].max_dist, false);
+        hs[i].begin = static_cast<uint32_t>(begin);
+        hs[i].count = static_cast<uint32_t>(sets[i].count);
+        begin += sets[i].count;
+        h.max_dist = std::max(h.max_dist, sets[i].max_dist);
+    }
+    std::memcpy(ws.h_batch, &h, sizeof h);
+    const BatchHeader* d_hdr = reinterpret_cast<const BatchHeader*>(ws.batch.p);
+    const SetDesc* d_sets = reinterpret_cast<const SetDesc*>(ws.batch.p + sizeof(BatchHeader));
+    for (int attempt = 0; attempt < 4; attempt++) {
+        ensure_capacity(ix, ws, n, true, st);
+        // the graph covers every batch up to the capacities it was captured with
+        if (!ws.graph || ws.graph_epoch != ws.epoch || ws.graph_tuning != ix->tuning_version) {
+            if (ws.graph) cudaGraphExecDestroy(ws.graph);
+            ws.graph = nullptr;
+            ISSL_CUDA(cudaStreamSynchronize(st));
+            RunSpec R;
+            R.qsig = ws.qsig.p;
+            R.n = ws.q_cap;
+            R.P = make_params(ISSL_METHOD_MIT_AND_CFD, 50.0, kMaxDist, false);
+            R.hdr = d_hdr;
+            R.sets = d_sets;
+            R.mit = ws.out_mit.p;
+            R.cfd = ws.out_cfd.p;
+            R.code = ws.out_code.p;
+            R.count = ws.out_count.p;
+            R.events = false;
+            cudaGraph_t g = nullptr;
+            ISSL_CUDA(cudaStreamBeginCapture(ws.cap_stream, cudaStreamCaptureModeThreadLocal));
+            uint64_t k = 0;
+            try {
+                k = enqueue_pipeline(ix, ws, R, ws.cap_stream);
+            } catch (...) {
+                cudaStreamEndCapture(ws.cap_stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            ISSL_CUDA(cudaStreamEndCapture(ws.cap_stream, &g));
+            const cudaError_t e = cudaGraphInstantiate(&ws.graph, g, 0);
+            cudaGraphDestroy(g);
+            ISSL_CUDA(e);
+            ws.graph_epoch = ws.epoch;
+            ws.graph_tuning = ix->tuning_version;
+            ws.graph_kernels = k;
+        }
+        ISSL_CUDA(cudaMemcpyAsync(ws.batch.p, ws.h_batch, table_bytes, cudaMemcpyHostToDevice, st));
+        ISSL_CUDA(cudaEventRecord(b->ev0, st));
+        ISSL_CUDA(cudaGraphLaunch(ws.graph, st));
+        ISSL_CUDA(cudaEventRecord(b->ev1, st));
+        if (check_and_grow(ws, st)) {
+            float total = 0.f;
+            cudaEventElapsedTime(&total, b->ev0, b->ev1);
+            fill_stats(ws, 0.f, total, ws.graph_kernels, b->stats);
+            return;
+        }
+    }
+    throw Error(ISSL_ERR_NOMEM, "scoring workspace kept overflowing");
+}
+
+void check_sets(uint64_t n, const issl_guide_set* sets, size_t n_sets) {
+    ISSL_REQUIRE(n_sets >= 1 && n_sets <= kMaxSets, ISSL_ERR_ARG, "a batch holds 1..65535 guide sets");
+    ISSL_REQUIRE(sets, ISSL_ERR_ARG, "issl_batch_score: null set table");
+    uint64_t total = 0;
+    for (size_t i = 0; i < n_sets; i++) {
+        make_params(sets[i].method, sets[i].threshold, sets[i].max_dist, false);  // validates
+        total += sets[i].count;
+    }
+    ISSL_REQUIRE(total == n, ISSL_ERR_ARG, "the set counts must add up to the number of guides");
 }
 
 }  // namespace
@@ -1376,7 +1697,7 @@ int issl_score_device(issl_index* ix, const uint64_t* d_sigs, size_t n, int meth
         }
         ISSL_REQUIRE(n < (1ull << issl::kGuideBits) && n * ix->n_slices < 0xFFFFFFFFull, ISSL_ERR_ARG,
                      "too many guides in one call (at most 2^26 and 2^32 guide-slice pairs)");
-        issl::run_scoring(ix, d_sigs, n, P, d_mit, d_cfd, d_code, d_count, d_distinct, st, true);
+        issl::run_scoring(ix, d_sigs, n, P, d_mit, d_cfd, d_code, d_count, d_distinct, st);
     });
 }
 
@@ -1397,7 +1718,7 @@ static int score_host_common(issl_index* ix, const char* seqs, size_t stride, co
         }
         ISSL_REQUIRE(n < (1ull << issl::kGuideBits) && n * ix->n_slices < 0xFFFFFFFFull, ISSL_ERR_ARG,
                      "too many guides in one call (at most 2^26 and 2^32 guide-slice pairs)");
-        issl::ensure_capacity(ix, ws, n, st);
+        issl::ensure_capacity(ix, ws, n, false, st);
         if (seqs) {
             const size_t bytes = (n - 1) * stride + issl::kSeqLen;
             if (ws.ascii_cap < bytes) {
@@ -1411,7 +1732,7 @@ static int score_host_common(issl_index* ix, const char* seqs, size_t stride, co
             ISSL_CUDA(cudaMemcpyAsync(ws.qsig.p, sigs, n * 8, cudaMemcpyHostToDevice, st));
         }
         issl::run_scoring(ix, ws.qsig.p, n, P, ws.out_mit.p, ws.out_cfd.p, ws.out_code.p, ws.out_count.p,
-                          distinct ? ws.out_distinct.p : nullptr, st, true);
+                          distinct ? ws.out_distinct.p : nullptr, st);
         if (mit) ISSL_CUDA(cudaMemcpyAsync(mit, ws.out_mit.p, n * 8, cudaMemcpyDeviceToHost, st));
         if (cfd) ISSL_CUDA(cudaMemcpyAsync(cfd, ws.out_cfd.p, n * 8, cudaMemcpyDeviceToHost, st));
         ISSL_CUDA(cudaMemcpyAsync(code, ws.out_code.p, n, cudaMemcpyDeviceToHost, st));
@@ -1430,6 +1751,107 @@ int issl_score(issl_index* ix, const char* seqs, size_t stride, size_t n, int me
 int issl_score_sigs(issl_index* ix, const uint64_t* sigs, size_t n, int method, double threshold, int max_dist,
                     double* mit, double* cfd, char* code, uint64_t* count, uint64_t* distinct) {
     return score_host_common(ix, nullptr, 0, sigs, n, method, threshold, max_dist, mit, cfd, code, count, distinct);
+}
+
+int issl_workspace_bytes(const issl_index* ix, uint64_t n, double candidates_per_guide, uint64_t* bytes) {
+    return guarded([&] {
+        ISSL_REQUIRE(ix && bytes && candidates_per_guide >= 0, ISSL_ERR_ARG, "issl_workspace_bytes: bad argument");
+        uint64_t fixed, per_guide, per_candidate;
+        issl::workspace_model(ix, &fixed, &per_guide, &per_candidate);
+        *bytes = fixed + n * per_guide +
+                 static_cast<uint64_t>(static_cast<double>(n) * candidates_per_guide) * per_candidate;
+    });
+}
+
+int issl_get_tuning(const issl_index* ix, issl_tuning* out) {
+    return guarded([&] {
+        ISSL_REQUIRE(ix && out, ISSL_ERR_ARG, "issl_get_tuning: null argument");
+        *out = ix->tuning;
+    });
+}
+
+int issl_set_tuning(issl_index* ix, const issl_tuning* t) {
+    return guarded([&] {
+        ISSL_REQUIRE(ix && t, ISSL_ERR_ARG, "issl_set_tuning: null argument");
+        for (uint32_t c : t->chunk)
+            ISSL_REQUIRE(c == 256 || c == 512 || c == 1024, ISSL_ERR_ARG, "tuning: unit sizes are 256, 512 or 1024");
+        ISSL_REQUIRE(t->stages >= 2 && t->stages <= static_cast<uint32_t>(issl::kMaxStages), ISSL_ERR_ARG,
+                     "tuning: stages must be 2..4");
+        ISSL_REQUIRE(t->blocks_per_sm <= 32, ISSL_ERR_ARG, "tuning: blocks_per_sm must be 0..32");
+        ix->tuning = *t;
+        ix->tuning_version++;
+    });
+}
+
+int issl_batch_create(issl_index* ix, issl_batch** out) {
+    return guarded([&] {
+        ISSL_REQUIRE(ix && out, ISSL_ERR_ARG, "issl_batch_create: null argument");
+        *out = nullptr;
+        ISSL_CUDA(cudaSetDevice(ix->device));
+        auto b = std::make_unique<issl_batch>();
+        b->ix = ix;
+        b->ws = issl::new_workspace(ix);
+        ISSL_CUDA(cudaEventCreate(&b->ev0));
+        ISSL_CUDA(cudaEventCreate(&b->ev1));
+        *out = b.release();
+    });
+}
+
+void issl_batch_destroy(issl_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->ix->device);
+    delete b;
+}
+
+int issl_batch_score(issl_batch* b, const uint64_t* d_sigs, size_t n, const issl_guide_set* sets, size_t n_sets,
+                     double* d_mit, double* d_cfd, char* d_code, uint64_t* d_count, void* stream) {
+    return guarded([&] {
+        ISSL_REQUIRE(b && (d_sigs || n == 0) && d_code, ISSL_ERR_ARG, "issl_batch_score: null argument");
+        issl::check_sets(n, sets, n_sets);
+        if (n == 0) return;
+        ISSL_REQUIRE(n < (1ull << issl::kGuideBits) && n * b->ix->n_slices < 0xFFFFFFFFull, ISSL_ERR_ARG,
+                     "too many guides in one batch (at most 2^26 and 2^32 guide-slice pairs)");
+        ISSL_CUDA(cudaSetDevice(b->ix->device));
+        issl::Workspace& ws = *b->ws;
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ws.own_stream;
+        issl::ensure_capacity(b->ix, ws, n, true, st);
+        if (d_sigs != ws.qsig.p) ISSL_CUDA(cudaMemcpyAsync(ws.qsig.p, d_sigs, n * 8, cudaMemcpyDeviceToDevice, st));
+        issl::run_batch(b, n, sets, n_sets, st);
+        if (d_mit) ISSL_CUDA(cudaMemcpyAsync(d_mit, ws.out_mit.p, n * 8, cudaMemcpyDeviceToDevice, st));
+        if (d_cfd) ISSL_CUDA(cudaMemcpyAsync(d_cfd, ws.out_cfd.p, n * 8, cudaMemcpyDeviceToDevice, st));
+        ISSL_CUDA(cudaMemcpyAsync(d_code, ws.out_code.p, n, cudaMemcpyDeviceToDevice, st));
+        if (d_count) ISSL_CUDA(cudaMemcpyAsync(d_count, ws.out_count.p, n * 8, cudaMemcpyDeviceToDevice, st));
+        ISSL_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int issl_batch_score_host(issl_batch* b, const uint64_t* sigs, size_t n, const issl_guide_set* sets, size_t n_sets,
+                          double* mit, double* cfd, char* code, uint64_t* count) {
+    return guarded([&] {
+        ISSL_REQUIRE(b && (sigs || n == 0) && code, ISSL_ERR_ARG, "issl_batch_score_host: null argument");
+        issl::check_sets(n, sets, n_sets);
+        if (n == 0) return;
+        ISSL_REQUIRE(n < (1ull << issl::kGuideBits) && n * b->ix->n_slices < 0xFFFFFFFFull, ISSL_ERR_ARG,
+                     "too many guides in one batch (at most 2^26 and 2^32 guide-slice pairs)");
+        ISSL_CUDA(cudaSetDevice(b->ix->device));
+        issl::Workspace& ws = *b->ws;
+        cudaStream_t st = ws.own_stream;
+        issl::ensure_capacity(b->ix, ws, n, true, st);
+        ISSL_CUDA(cudaMemcpyAsync(ws.qsig.p, sigs, n * 8, cudaMemcpyHostToDevice, st));
+        issl::run_batch(b, n, sets, n_sets, st);
+        if (mit) ISSL_CUDA(cudaMemcpyAsync(mit, ws.out_mit.p, n * 8, cudaMemcpyDeviceToHost, st));
+        if (cfd) ISSL_CUDA(cudaMemcpyAsync(cfd, ws.out_cfd.p, n * 8, cudaMemcpyDeviceToHost, st));
+        ISSL_CUDA(cudaMemcpyAsync(code, ws.out_code.p, n, cudaMemcpyDeviceToHost, st));
+        if (count) ISSL_CUDA(cudaMemcpyAsync(count, ws.out_count.p, n * 8, cudaMemcpyDeviceToHost, st));
+        ISSL_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int issl_batch_stats(const issl_batch* b, issl_score_stats* out) {
+    return guarded([&] {
+        ISSL_REQUIRE(b && out, ISSL_ERR_ARG, "issl_batch_stats: null argument");
+        *out = b->stats;
+    });
 }
 
 int issl_last_stats(const issl_index* ix, issl_score_stats* out) {

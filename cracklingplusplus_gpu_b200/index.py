@@ -7,7 +7,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from ._lib import CLI_METHODS, OT_METHODS, IndexInfo, ScoreStats, SynthSpecC, check, lib
+from ._lib import CLI_METHODS, OT_METHODS, IndexInfo, ScoreStats, SynthSpecC, TuneReport, Tuning, check, lib
 
 
 def _u64(a) -> C.POINTER(C.c_uint64):
@@ -138,6 +138,24 @@ class Index:
         out = ScoreStats()
         check(lib().issl_last_stats(self._h, C.byref(out)))
         return out
+
+    # ---- tuning -----------------------------------------------------------------------------
+    def get_tuning(self) -> Tuning:
+        out = Tuning()
+        check(lib().issl_get_tuning(self._h, C.byref(out)))
+        return out
+
+    def set_tuning(self, chunk=(1024, 1024, 1024), stages: int = 3, blocks_per_sm: int = 0) -> None:
+        t = Tuning((C.c_uint32 * 3)(*chunk), stages, blocks_per_sm)
+        check(lib().issl_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, d_sigs: int, n: int, method="and", threshold: float = 75.0, max_dist: int = 4,
+                 cache_path: Optional[str] = None):
+        """Sweeps the scan tuning on a device-resident sample; returns (Tuning, TuneReport)."""
+        t, r = Tuning(), TuneReport()
+        check(lib().issl_autotune(self._h, C.c_void_p(d_sigs), n, _method(method), threshold, max_dist,
+                                  cache_path.encode() if cache_path else None, C.byref(t), C.byref(r)))
+        return t, r
 
     # ---- scoring --------------------------------------------------------------------------
     def score(self, guides, method="and", threshold: float = 75.0, max_dist: int = 4,

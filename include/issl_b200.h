@@ -147,9 +147,143 @@ int issl_score_device_static(issl_index* index, const uint64_t* d_sigs, size_t n
 typedef struct {
     double scan_ms, total_ms;
     uint64_t probes, buckets_scanned, entries_scanned, units, hits, scan_bytes;
-    uint64_t launches;  /* kernels this library launched for the call */
+    uint64_t launches;          /* kernels this library launched for the call */
+    uint64_t class_probes[3];   /* probes into buckets of < 64, 64..4095 and >= 4096 entries */
+    uint64_t candidates;        /* candidate slots the scan wrote, before the ownership rule */
 } issl_score_stats;
+
+/* Modelled device bytes of one scoring workspace (the per-call buffers of issl_score*,
+ * a batch context or a server slot) holding n guides, when the scan finds `candidates_per_guide`
+ * candidate sites per guide (64 is the library's first guess). No counterpart in the reference.
+ * The server admits requests by this footprint. */
+int issl_workspace_bytes(const issl_index* index, uint64_t n, double candidates_per_guide, uint64_t* bytes);
 int issl_last_stats(const issl_index* index, issl_score_stats* out);
+
+/* ---- scan tuning and autotuning ------------------------------------------------------------
+ * No counterpart in the reference (its CPU loop has no tiles). The scan streams each probed
+ * bucket in units of up to 1024 list positions shared by up to 32 guides; `chunk` sets the unit
+ * size per bucket-size class (smaller units spread a heavy bucket over more warps), `stages`
+ * the depth of each warp's asynchronous copy ring, `blocks_per_sm` the persistent grid. Results
+ * do not depend on the tuning; only speed does. */
+typedef struct {
+    uint32_t chunk[3];       /* buckets of < 64, 64..4095, >= 4096 entries: 256, 512 or 1024 */
+    uint32_t stages;         /* 2..4 (default 3) */
+    uint32_t blocks_per_sm;  /* 0 = as many as fit (default) */
+} issl_tuning;
+int issl_get_tuning(const issl_index* index, issl_tuning* out);
+int issl_set_tuning(issl_index* index, const issl_tuning* tuning);
+
+typedef struct {
+    double default_ms;       /* pipeline time with the tuning the index had */
+    double best_ms;          /* pipeline time with the chosen tuning */
+    uint32_t configs_timed;  /* tunings measured (0 when the result came from the cache) */
+    uint32_t from_cache;
+    uint64_t class_probes[3];/* bucket-size class histogram of the sample's probes */
+} issl_tune_report;
+
+/* Sweeps the tuning on a sample workload (d_sigs: n guides in device memory, scored with the
+ * given method / threshold / max_dist), starting from the current tuning: staging depth first,
+ * then the unit size of each bucket-size class that the sample's probes reach (heaviest class
+ * first), then blocks per SM, keeping a change only when the pipeline gets faster by more than
+ * 2%. The winner is applied to the index and, when cache_path is not NULL, appended there under
+ * a key made of the GPU name, the index geometry and the sample size; a later call with the
+ * same key reads it back without timing. */
+int issl_autotune(issl_index* index, const uint64_t* d_sigs, size_t n, int method, double threshold,
+                  int max_dist, const char* cache_path, issl_tuning* out, issl_tune_report* report);
+
+/* ---- batched scoring -----------------------------------------------------------------------
+ * No counterpart in the reference, which scores one query file per process. Many independent
+ * guide sets, each with its own method, threshold and mismatch bound, are scored in one pass:
+ * the whole pipeline is captured once into a CUDA graph and replayed for every batch that fits
+ * its capacities (it is re-captured when a capacity grows or the tuning changes). Every guide
+ * gets exactly the result issl_score_device gives it in a call of its own. */
+typedef struct {
+    uint64_t count;      /* guides in the set; sets follow each other in the signature array */
+    int method;          /* ISSL_METHOD_* */
+    int max_dist;        /* 0..4 */
+    double threshold;
+} issl_guide_set;
+
+typedef struct issl_batch issl_batch;
+
+/* A batch context: its own workspace and graph on the index's device (one per thread). */
+int issl_batch_create(issl_index* index, issl_batch** out);
+void issl_batch_destroy(issl_batch* batch);
+
+/* Scores n guides (device memory, packed signatures) split into n_sets consecutive sets
+ * (host array; counts sum to n; at most 65535 sets and 2^26 guides). Outputs are device
+ * buffers of n entries (any may be NULL except d_code); counts are per guide as in issl_score.
+ * Work is enqueued on `stream` (NULL = the batch's own stream); the call returns when the
+ * results are in the output buffers. */
+int issl_batch_score(issl_batch* batch, const uint64_t* d_sigs, size_t n, const issl_guide_set* sets,
+                     size_t n_sets, double* d_mit_score, double* d_cfd_score, char* d_code,
+                     uint64_t* d_count, void* stream);
+
+/* Same with host buffers: signatures in, scores out. */
+int issl_batch_score_host(issl_batch* batch, const uint64_t* sigs, size_t n, const issl_guide_set* sets,
+                          size_t n_sets, double* mit_score, double* cfd_score, char* code, uint64_t* count);
+
+/* Timing and counters of the last batch: total_ms is the graph replay (device time), launches
+ * the kernels in the graph. */
+int issl_batch_stats(const issl_batch* batch, issl_score_stats* out);
+
+/* ---- serving ---------------------------------------------------------------------------------
+ * No counterpart in the reference (a CLI run per query file). A request loop in front of the
+ * resident index: guide-set requests (each with its own method / threshold / mismatch bound)
+ * are queued as they arrive; each of n_slots worker slots, with its own workspace and captured
+ * graph, repeatedly takes the waiting requests in arrival order and scores them together as one
+ * batch. A batch is admitted while it stays within max_batch_guides and its device-memory
+ * footprint (issl_workspace_bytes, with a candidates-per-guide estimate that grows with what
+ * batches produced) stays within the slot's share of the device memory that was free at creation
+ * minus headroom_bytes. Batches of different slots overlap on the GPU. Every request gets exactly
+ * the result a call of its own gives. */
+typedef struct {
+    uint32_t n_slots;           /* batches on the GPU at once (0 = 3) */
+    uint32_t max_wait_us;       /* a free slot waits this long for more arrivals before scoring (0) */
+    uint64_t max_batch_guides;  /* guides per batch, and per request at most (0 = 131072) */
+    uint64_t headroom_bytes;    /* device memory left free beside the index and the slots (0 = 16 GiB) */
+} issl_server_config;
+
+typedef struct {
+    double queue_ms;            /* submit -> admitted into a batch */
+    double service_ms;          /* admitted -> results ready */
+    double latency_ms;          /* submit -> results ready */
+    uint64_t batch_guides;      /* guides in the request's batch */
+    uint32_t batch_requests;    /* requests in the request's batch */
+    uint32_t slot;
+} issl_request_info;
+
+typedef struct {
+    uint64_t requests, guides, batches;   /* completed since creation or the last reset */
+    double p50_ms, p99_ms, max_ms;        /* request latency, submit -> results ready */
+    double mean_batch_guides;
+    uint32_t slots, peak_in_flight;       /* peak_in_flight: most batches on the GPU at once */
+    uint64_t slot_budget_bytes, peak_batch_bytes;
+} issl_server_summary;
+
+typedef struct issl_server issl_server;
+
+/* Starts the slots (NULL config = defaults). Fails with ISSL_ERR_NOMEM when the free device
+ * memory minus the headroom cannot hold one slot's workspace. */
+int issl_server_create(issl_index* index, const issl_server_config* config, issl_server** out);
+
+/* Queues n guides (host memory, packed signatures; copied) as one request and returns its ticket
+ * at once. ISSL_ERR_ARG for a bad method / max_dist or n above max_batch_guides, ISSL_ERR_BUSY when
+ * the request alone needs more device memory than a slot may use. */
+int issl_server_submit(issl_server* server, const uint64_t* sigs, size_t n, int method, double threshold,
+                       int max_dist, uint64_t* ticket);
+
+/* Waits up to timeout_ms (< 0: no limit) for the request and copies its n results (any output
+ * may be NULL; info may be NULL). ISSL_ERR_TIMEOUT when not finished yet (the ticket stays
+ * valid); otherwise the ticket is consumed. */
+int issl_server_wait(issl_server* server, uint64_t ticket, int timeout_ms, double* mit_score,
+                     double* cfd_score, char* code, uint64_t* count, issl_request_info* info);
+
+/* Latency percentiles and counters of the completed requests; reset != 0 starts a new window. */
+int issl_server_stats(issl_server* server, issl_server_summary* out, int reset);
+
+/* Finishes every submitted request, then stops the slots and frees their workspaces. */
+void issl_server_destroy(issl_server* server);
 
 /* ---- synthetic workloads (benchmarks and tests) ------------------------------------------ */
 typedef struct {
