@@ -69,6 +69,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default scan tuning (no autotune sweep)")
+    ap.add_argument("--form", default="plain",
+                    help="plain (default: the headline line), or batched and/or served (comma-separated): the "
+                         "slice-10-37 forms, one JSON line each")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the served-load run")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="request arrivals per second (Poisson)")
     return ap.parse_args()
 
 
@@ -224,7 +229,7 @@ def run_ours(args):
     tuning = None
     if not args.no_tune:
         t, rep = ix.autotune(d_q.data_ptr(), nq, method_id, thr, md)
-        tuning = {"chunk": list(t.chunk), "stages": t.stages, "blocks_per_sm": t.blocks_per_sm,
+        tuning = {"chunk": list(t.chunk), "stages": t.stages, "blocks_per_sm": t.blocks_per_sm, "first_wave": t.first_wave,
                   "default_ms": rep.default_ms, "tuned_ms": rep.best_ms, "configs_timed": rep.configs_timed,
                   "class_probes": list(rep.class_probes)}
 
@@ -384,12 +389,246 @@ def run_reference(args):
     }), flush=True)
 
 
+# ---- batched and served forms (300M-site slice-10-37 index) -----------------------------------
+FORMS = {
+    "n_sites": 300_000_000,
+    "slice_config": "slice-10-37",
+    "repeat_frac": 0.05,
+    "repeat_seeds": 10_000,
+    "repeat_lambda": 2.0,
+    "repeat_query_frac": 0.2,
+    "seed": 1236,
+    "pool": 2_000_000,
+}
+BATCHED = {"workload": "issl-score batched: 300M-site slice-10-37 index, 256 guide sets of log-uniform size "
+                       "10..50,000 (20% repeat-derived guides), MIT+CFD 'and', threshold 75, max 4 mismatches",
+           "n_sets": 256, "set_min": 10, "set_max": 50_000, "method": "and", "threshold": 75.0, "max_dist": 4}
+SERVED = {"workload": "issl-score served: 300M-site slice-10-37 index, Poisson arrivals, log-normal request sizes "
+                      "(median 1,000, sigma 1.5, cap 100,000), methods MIT / CFD / MIT+CFD, thresholds 50/75/90, "
+                      "max 4 mismatches, 16 GB device-memory headroom",
+          "median": 1000, "sigma": 1.5, "cap": 100_000, "methods": ["mit", "cfd", "and"], "thresholds": [50.0, 75.0, 90.0],
+          "headroom_gb": 16, "slots": 3, "max_batch_guides": 131072}
+
+
+def run_forms(args, forms):
+    import torch
+    import cracklingplusplus_gpu_b200 as pkg
+    from cracklingplusplus_gpu_b200 import build
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    build.build()
+    torch.cuda.set_device(local)
+    n_sites = args.sites or FORMS["n_sites"]
+    pool = args.queries or FORMS["pool"]
+    spec = pkg.SynthSpec(seed=FORMS["seed"], n_sites=n_sites, slice_config=FORMS["slice_config"], n_queries=pool,
+                         repeat_frac=FORMS["repeat_frac"], n_repeat_seeds=FORMS["repeat_seeds"],
+                         repeat_lambda=FORMS["repeat_lambda"], repeat_query_frac=FORMS["repeat_query_frac"])
+    t0 = time.time()
+    ix, q = pkg.Index.synth(spec, device=local)
+    gen_s = time.time() - t0
+    base = {"n_sites": n_sites, "slice_config": FORMS["slice_config"], "seed": FORMS["seed"],
+            "repeat_query_frac": FORMS["repeat_query_frac"], "generation_s": gen_s}
+    log(f"index: {n_sites} sites, {FORMS['slice_config']}, {pool} pool guides, generated in {gen_s:.1f} s")
+    if "batched" in forms:
+        print(json.dumps(bench_batched(args, pkg, ix, q, base)), flush=True)
+        ix.trim()  # the plain calls' workspace is not needed by the server
+    if "served" in forms:
+        print(json.dumps(bench_served(args, pkg, ix, q, base)), flush=True)
+    ix.close()
+
+
+def log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
+def bench_batched(args, pkg, ix, q, base):
+    """256 sets in one graph replay against the plain form (one pipeline per set) on the same guides."""
+    import torch
+    rng = np.random.default_rng(FORMS["seed"])
+    sizes = np.exp(rng.uniform(np.log(BATCHED["set_min"]), np.log(BATCHED["set_max"]), BATCHED["n_sets"])).astype(int)
+    while sizes.sum() > len(q):
+        sizes = (sizes * 0.9).astype(int) + 1
+    n = int(sizes.sum())
+    meth = pkg.CLI_METHODS[BATCHED["method"]]
+    thr, md = BATCHED["threshold"], BATCHED["max_dist"]
+    sets = [(int(k), meth, thr, md) for k in sizes]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.Stream(device=dev)
+    d_q = torch.from_numpy(np.ascontiguousarray(q[:n]).view(np.int64)).to(dev)
+    d_mit = torch.empty(n, dtype=torch.float64, device=dev)
+    d_cfd = torch.empty(n, dtype=torch.float64, device=dev)
+    d_code = torch.empty(n, dtype=torch.uint8, device=dev)
+    d_cnt = torch.empty(n, dtype=torch.int64, device=dev)
+    tuning = None
+    if not args.no_tune:
+        t, rep = ix.autotune(d_q.data_ptr(), n, meth, thr, md)
+        tuning = {"chunk": list(t.chunk), "stages": t.stages, "blocks_per_sm": t.blocks_per_sm, "first_wave": t.first_wave,
+                  "default_ms": rep.default_ms, "tuned_ms": rep.best_ms, "class_probes": list(rep.class_probes)}
+    ix.trim()  # the sweep's workspace; the batch context holds its own
+    bt = pkg.Batch(ix)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(step, steps, warmup):
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / steps
+
+    def batched():
+        bt.score_device(d_q.data_ptr(), n, sets, d_mit.data_ptr(), d_cfd.data_ptr(), d_code.data_ptr(),
+                        d_cnt.data_ptr(), stream.cuda_stream)
+
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+
+    def per_set():  # the plain form: one pipeline (one query file) per set
+        for i in range(len(sizes)):
+            a = int(offs[i])
+            ix.score_device(d_q.data_ptr() + 8 * a, int(sizes[i]), meth, thr, md, d_mit.data_ptr() + 8 * a,
+                            d_cfd.data_ptr() + 8 * a, d_code.data_ptr() + a, d_cnt.data_ptr() + 8 * a, 0,
+                            stream.cuda_stream)
+
+    def one_call():
+        ix.score_device(d_q.data_ptr(), n, meth, thr, md, d_mit.data_ptr(), d_cfd.data_ptr(), d_code.data_ptr(),
+                        d_cnt.data_ptr(), 0, stream.cuda_stream)
+
+    log(f"batched: {n} guides in {len(sizes)} sets; tuning {tuning}")
+    steps = max(3, args.steps // 10)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        ms_batched = timed(batched, steps, max(args.warmup, 3))
+    st = bt.stats()
+    code_b = d_code.cpu().numpy().copy()
+    mit_b = d_mit.cpu().numpy().copy()
+    log(f"batched: {ms_batched:.2f} ms per replay")
+    # end to end: host signatures in, host results out, through issl_batch_score_host
+    hq = np.ascontiguousarray(q[:n])
+    t0 = time.perf_counter()
+    for _ in range(2):
+        bt.score(hq, sets)
+    e2e_s = (time.perf_counter() - t0) / 2
+    bt.close()  # the plain calls below use the index's own workspace
+    ms_sets = timed(per_set, max(2, steps // 3), 1)
+    equal = bool(np.array_equal(code_b, d_code.cpu().numpy()) and np.array_equal(mit_b, d_mit.cpu().numpy()))
+    ms_one = timed(one_call, steps, 2)
+    one = ix.last_stats()
+    peak, peak_kind = measured_peaks()
+    return {
+        "metric": "guides/sec, batched form (256 guide sets, one graph replay)", "value": n / (ms_batched / 1e3),
+        "unit": "guides/s", "n_gpus": 1, "steps": steps, "ms_per_step": ms_batched, "higher_is_better": True,
+        "dtype": "u32/u64 integer scan, f64 sums", "data": "synthetic (seeded, generated on device)",
+        "config": dict(BATCHED, **base, n_guides=n),
+        "plain_per_set": {"value": n / (ms_sets / 1e3), "ms_per_step": ms_sets,
+                          "note": "one issl_score_device pipeline per set, same guides and stream"},
+        "plain_one_call": {"value": n / (ms_one / 1e3), "ms_per_step": ms_one,
+                           "note": "all guides in one plain call (one parameter set)"},
+        "batched_equals_per_set": equal,
+        "e2e": {"value": n / e2e_s, "unit": "guides/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 25 * n},
+        "gpu_launches_per_step": int(st.launches), "graph_replays_per_step": 1,
+        "scan": {"kernel_ms": one.scan_ms, "bytes_per_launch": one.scan_bytes,
+                 "achieved_gbs": one.scan_bytes / (one.scan_ms / 1e3) / 1e9 if one.scan_ms else None,
+                 "peak": peak, "peak_kind": peak_kind, "class_probes": list(one.class_probes)},
+        "owned_hits_per_step": int(st.hits), "tuning": tuning, "clocks": clocks.summary(),
+    }
+
+
+def bench_served(args, pkg, ix, q, base):
+    """Open-loop Poisson arrivals against the server; latency from submit to results ready."""
+    import queue
+    rng = np.random.default_rng(FORMS["seed"] + 1)
+    rate, seconds = args.serve_rate, args.serve_seconds
+    srv = pkg.Server(ix, n_slots=SERVED["slots"], max_batch_guides=SERVED["max_batch_guides"],
+                     headroom_bytes=SERVED["headroom_gb"] << 30)
+
+    def draw():
+        k = int(min(SERVED["cap"], max(1, round(rng.lognormal(np.log(SERVED["median"]), SERVED["sigma"])))))
+        a = int(rng.integers(0, len(q) - k))
+        return (q[a:a + k], SERVED["methods"][rng.integers(3)], SERVED["thresholds"][rng.integers(3)], 4)
+
+    # warm-up: every slot reaches its full capacity (buffers and captured graph) before timing
+    w = min(SERVED["max_batch_guides"], len(q))
+    warm = [srv.submit(q[:w], "and", 75.0, 4) for _ in range(2 * SERVED["slots"])]
+    for t in warm:
+        srv.wait(t)
+    srv.stats(reset=True)
+    log(f"served: warm, {seconds:.0f} s at {rate:.0f} requests/s")
+    tickets: "queue.Queue" = queue.Queue()
+    replies = []
+
+    def collector():
+        while True:
+            item = tickets.get()
+            if item is None:
+                return
+            t, k, req = item
+            r = srv.wait(t)
+            replies.append((k, r.info.latency_ms, r.info.queue_ms, r.info.batch_requests, req, r.result))
+
+    cols = [threading.Thread(target=collector) for _ in range(4)]
+    for c in cols:
+        c.start()
+    start = time.perf_counter()
+    next_t = start
+    n_req = offered = 0
+    sample_reqs = []
+    while True:
+        next_t += rng.exponential(1.0 / rate)
+        if next_t - start > seconds:
+            break
+        delay = next_t - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        req = draw()
+        t = srv.submit(*req)
+        n_req += 1
+        offered += len(req[0])
+        tickets.put((t, len(req[0]), req if len(sample_reqs) < 40 and n_req % 25 == 0 else None))
+    for _ in cols:
+        tickets.put(None)
+    for c in cols:
+        c.join()
+    wall = time.perf_counter() - start
+    st = srv.stats()
+    srv.close()
+    lat = np.array([r[1] for r in replies])
+    k = np.array([r[0] for r in replies])
+    one_k = lat[(k >= 500) & (k <= 2000)]
+    # alone-vs-mixed check on a sample of the served requests
+    mixed_ok, checked = True, 0
+    for _, _, _, nb, req, res in replies:
+        if req is None:
+            continue
+        alone = ix.score(req[0], req[1], req[2], max_dist=req[3], distinct=False)
+        mixed_ok &= alone.code == res.code and np.array_equal(alone.mit, res.mit) and np.array_equal(alone.cfd, res.cfd)
+        checked += 1
+    return {
+        "metric": "served latency p99 (ms), MIT/CFD <=4 mm, 300M-site slice-10-37 index",
+        "value": float(np.percentile(lat, 99)), "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "p99_ms_1k_guide_requests": float(np.percentile(one_k, 99)) if len(one_k) else None,
+        "p50_ms_1k_guide_requests": float(np.percentile(one_k, 50)) if len(one_k) else None,
+        "requests": int(len(lat)), "throughput_guides_per_s": float(k.sum() / wall),
+        "offered_guides_per_s": offered / seconds, "rate_req_per_s": rate, "seconds": seconds,
+        "batches": int(st.batches), "mean_batch_guides": st.mean_batch_guides, "peak_in_flight": int(st.peak_in_flight),
+        "slots": int(st.slots), "slot_budget_bytes": int(st.slot_budget_bytes), "peak_batch_bytes": int(st.peak_batch_bytes),
+        "mixed_equals_alone": {"checked": checked, "equal": bool(mixed_ok)},
+        "data": "synthetic (seeded, generated on device)", "config": dict(SERVED, **base),
+    }
+
+
 def main():
     args = parse()
+    forms = [f.strip() for f in args.form.split(",") if f.strip()]
     if args.impl == "reference":
         run_reference(args)
-    else:
+    elif forms == ["plain"]:
         run_ours(args)
+    else:
+        run_forms(args, forms)
 
 
 if __name__ == "__main__":

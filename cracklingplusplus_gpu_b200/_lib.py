@@ -27,7 +27,7 @@ class IsslError(RuntimeError):
 class IndexInfo(C.Structure):
     _fields_ = [("n_sites", C.c_uint64), ("seq_len", C.c_uint64), ("n_slices", C.c_uint64),
                 ("n_buckets", C.c_uint64), ("device_bytes", C.c_uint64), ("device", C.c_int),
-                ("min_width", C.c_int), ("max_width", C.c_int)]
+                ("min_width", C.c_int), ("max_width", C.c_int), ("entry_bytes", C.c_int)]
 
 
 class ScoreStats(C.Structure):
@@ -39,11 +39,12 @@ class ScoreStats(C.Structure):
 
 class Tuning(C.Structure):
     """issl_tuning: scan unit size per bucket-size class (<64, 64..4095, >=4096 entries),
-    staging depth, scan blocks per SM (0 = as many as fit)."""
-    _fields_ = [("chunk", C.c_uint32 * 3), ("stages", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
+    staging depth, scan blocks per SM (0 = as many as fit), slices of the first wave."""
+    _fields_ = [("chunk", C.c_uint32 * 3), ("stages", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("first_wave", C.c_uint32)]
 
     def as_tuple(self):
-        return (tuple(self.chunk), self.stages, self.blocks_per_sm)
+        return (tuple(self.chunk), self.stages, self.blocks_per_sm, self.first_wave)
 
 
 class TuneReport(C.Structure):
@@ -120,6 +121,7 @@ SIGNATURES = [
                                         u64p]),
     ("issl_batch_stats", C.c_int, [vp, P(ScoreStats)]),
     ("issl_workspace_bytes", C.c_int, [vp, C.c_uint64, C.c_double, u64p]),
+    ("issl_index_trim", C.c_int, [vp]),
     ("issl_server_create", C.c_int, [vp, P(ServerConfig), P(vp)]),
     ("issl_server_submit", C.c_int, [vp, u64p, C.c_size_t, C.c_int, C.c_double, C.c_int, u64p]),
     ("issl_server_wait", C.c_int, [vp, C.c_uint64, C.c_int, f64p, f64p, C.c_char_p, u64p, P(RequestInfo)]),

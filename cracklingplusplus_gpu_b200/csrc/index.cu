@@ -3,10 +3,10 @@
 // Device layout (slice-major, list order of the reference file kept):
 //   sigs    [N]      u64  2-bit packed site signatures (the file's offtargets array)
 //   occ     [N]      u32  occurrence count per site (the high word of every list entry)
-//   ids     [S*N]    u32  site id per list entry (the low word of every list entry)
+//   ids     [S*N]    u32  packed list entry: site id + occurrence code (see IndexView); the one
+//                         random read per scored hit
 //   rbits   [...]    u32  residual codes (the site's bases outside the slice), bit-sliced in
 //                         blocks of 32 list positions, one word per residual bit
-//   srec    [N]      16 B site record (signature, occurrences): the one random read per scored hit
 //   offsets [G+1]    u64  bucket starts in global entry numbering (slice s, position j -> s*N + j);
 //                         buckets are numbered slice by slice, so off[g+1] - off[g] is always the
 //                         size of bucket g, across slice boundaries too
@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -71,6 +72,20 @@ std::vector<SliceGeom> make_geometry(const std::vector<uint64_t>& masks, uint64_
     return geom;
 }
 
+uint32_t choose_entry_words(uint64_t n_sites, uint64_t n_slices, uint64_t rbits_bytes) {
+    if (const char* e = std::getenv("ISSL_ENTRY_BYTES")) {
+        const std::string v(e);
+        ISSL_REQUIRE(v == "4" || v == "8", ISSL_ERR_ARG, "ISSL_ENTRY_BYTES must be 4 or 8");
+        return v == "8" ? 2u : 1u;
+    }
+    size_t free_b = 0, total_b = 0;
+    ISSL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    // what the 8-byte lists and the residual codes take, and what must stay free for scoring
+    const uint64_t need = n_sites * n_slices * 8 + rbits_bytes;
+    const uint64_t keep = std::max<uint64_t>(32ull << 30, total_b / 5);
+    return free_b > need + keep ? 2u : 1u;
+}
+
 uint64_t bitsliced_words(const std::vector<SliceGeom>& geom, uint64_t n_sites) {
     uint64_t w = 0;
     for (auto& g : geom) w += blocks_per_slice(n_sites) * g.wpb;
@@ -101,14 +116,16 @@ __global__ void k_offsets_from_sorted(const uint32_t* __restrict__ keys, uint64_
 
 // Bit-sliced residual codes of one slice: a warp per block of 32 list positions; lane e holds the
 // residual code of entry e and a ballot per bit collects word j = bit j of the 32 codes.
-__global__ void k_rbits(const uint32_t* __restrict__ ids, const uint64_t* __restrict__ sigs, uint64_t n,
-                        SliceGeom g, uint32_t* __restrict__ out) {
+// With 8-byte entries (ew == 2) it also stores each entry's residual code beside its packed id.
+__global__ void k_rbits(uint32_t* __restrict__ ids, uint32_t ew, uint32_t id_bits, const uint64_t* __restrict__ sigs,
+                        uint64_t n, SliceGeom g, uint32_t* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const uint64_t nblk = blocks_per_slice(n);
     for (uint64_t b = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5; b < nblk;
          b += (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5) {
         const uint64_t pos = b * 32 + lane;
-        const uint32_t r = pos < n ? slice_residual(sigs[ids[pos]], g) : 0u;
+        const uint32_t r = pos < n ? slice_residual(sigs[entry_id(ids[pos * ew], id_bits)], g) : 0u;
+        if (ew == 2 && pos < n) ids[pos * 2 + 1] = r;
         uint32_t mine = 0;
         const int nbits = 2 * g.rwidth;  // data words; word nbits is the zero padding word
         for (int j = 0; j < nbits; j++) {
@@ -135,8 +152,9 @@ enum : uint32_t { kBadId = 1u, kDupId = 2u, kOccMismatch = 4u, kWrongBucket = 8u
 // and the entry sits in the bucket of its own slice key.
 __global__ void k_split_entries(const uint64_t* __restrict__ entries, uint64_t j0, uint64_t cnt, uint64_t n_sites,
                                 int first_slice, SliceGeom g, const uint64_t* __restrict__ sigs,
-                                const uint32_t* __restrict__ bucket_of, uint32_t* __restrict__ ids_slice,
-                                uint32_t* __restrict__ occ, uint32_t* __restrict__ seen, uint32_t* flags) {
+                                const uint32_t* __restrict__ bucket_of, uint32_t* __restrict__ ids_slice, uint32_t ew,
+                                uint32_t id_bits, uint32_t occ_esc, uint32_t* __restrict__ occ,
+                                uint32_t* __restrict__ seen, uint32_t* flags) {
     for (uint64_t t = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; t < cnt;
          t += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint64_t e = entries[t];
@@ -145,10 +163,10 @@ __global__ void k_split_entries(const uint64_t* __restrict__ entries, uint64_t j
         const uint64_t j = j0 + t;
         if (id >= n_sites) {
             atomicOr(flags, kBadId);
-            ids_slice[j] = 0;
+            ids_slice[j * ew] = 0;
             continue;
         }
-        ids_slice[j] = static_cast<uint32_t>(id);
+        ids_slice[j * ew] = pack_entry(static_cast<uint32_t>(id), o, id_bits, occ_esc);
         const uint32_t bit = 1u << (id & 31);
         if (atomicOr(&seen[id >> 5], bit) & bit) atomicOr(flags, kDupId);
         if (first_slice)
@@ -159,18 +177,21 @@ __global__ void k_split_entries(const uint64_t* __restrict__ entries, uint64_t j
     }
 }
 
-__global__ void k_site_records(const uint64_t* __restrict__ sigs, const uint32_t* __restrict__ occ, uint64_t n,
-                               uint4* __restrict__ out) {
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        out[i] = make_uint4(static_cast<uint32_t>(sigs[i]), static_cast<uint32_t>(sigs[i] >> 32), occ[i], 0u);
-}
-
-__global__ void k_join_entries(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ occ, uint64_t cnt,
-                               uint64_t* __restrict__ out) {
+// packed entries of one slice from the sorted site ids
+__global__ void k_pack_entries(const uint32_t* __restrict__ sorted_ids, const uint32_t* __restrict__ occ, uint64_t cnt,
+                               uint32_t id_bits, uint32_t occ_esc, uint32_t ew, uint32_t* __restrict__ out) {
     for (uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; j < cnt;
          j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t id = ids[j];
+        const uint32_t id = sorted_ids[j];
+        out[j * ew] = pack_entry(id, occ[id], id_bits, occ_esc);
+    }
+}
+
+__global__ void k_join_entries(const uint32_t* __restrict__ ids, uint32_t ew, uint32_t id_bits,
+                               const uint32_t* __restrict__ occ, uint64_t cnt, uint64_t* __restrict__ out) {
+    for (uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; j < cnt;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t id = entry_id(ids[j * ew], id_bits);
         out[j] = (static_cast<uint64_t>(occ[id]) << 32) | id;
     }
 }
@@ -264,6 +285,7 @@ void load_stream(issl_index* ix, Source& src, int device) {
                  "Error reading index: header invalid (slice count " + std::to_string(ix->n_slices) + ")");
     ISSL_REQUIRE(ix->seq_len >= 1 && ix->seq_len <= 64, ISSL_ERR_FORMAT, "Error reading index: header invalid");
     const uint64_t N = ix->n_sites, S = ix->n_slices;
+    entry_packing(N, &ix->id_bits, &ix->occ_esc);
     cudaStream_t st;
     ISSL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     struct StreamGuard {
@@ -291,7 +313,9 @@ void load_stream(issl_index* ix, Source& src, int device) {
     ISSL_CUDA(cudaMemcpyAsync(ix->d_geom.p, ix->geom.data(), S * sizeof(SliceGeom), cudaMemcpyHostToDevice, st));
 
     ix->occ.reserve(N);
-    ix->ids.reserve(S * N);
+    ix->entry_words = choose_entry_words(N, S, (bitsliced_words(ix->geom, N) + 4) * 4);
+    const uint64_t ew = ix->entry_words;
+    ix->ids.reserve(S * N * ew);
     ix->rbits.reserve(bitsliced_words(ix->geom, N) + 4);
     ix->offsets.reserve(ix->n_buckets + 1);
     DevBuf<uint32_t> seen, bucket_of, flags;
@@ -330,12 +354,13 @@ void load_stream(issl_index* ix, Source& src, int device) {
             src.read(stg.h[b], cnt * 8, "reading slice contents failed");
             ISSL_CUDA(cudaMemcpyAsync(stg.d[b], stg.h[b], cnt * 8, cudaMemcpyHostToDevice, st));
             k_split_entries<<<grid_for(cnt), 256, 0, st>>>(stg.d[b], j, cnt, N, s == 0, g, ix->sigs.p, bucket_of.p,
-                                                           ix->ids.p + s * N, ix->occ.p, seen.p, flags.p);
+                                                           ix->ids.p + s * N * ew, ix->entry_words, ix->id_bits,
+                                                           ix->occ_esc, ix->occ.p, seen.p, flags.p);
             ISSL_CUDA(cudaEventRecord(stg.done[b], st));
             j += cnt;
         }
-        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(ix->ids.p + s * N, ix->sigs.p, N, g,
-                                                                    ix->rbits.p);
+        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(ix->ids.p + s * N * ew, ix->entry_words, ix->id_bits,
+                                                                    ix->sigs.p, N, g, ix->rbits.p);
         ISSL_CUDA(cudaGetLastError());
         uint32_t f = 0;
         ISSL_CUDA(cudaMemcpyAsync(&f, flags.p, 4, cudaMemcpyDeviceToHost, st));
@@ -348,9 +373,6 @@ void load_stream(issl_index* ix, Source& src, int device) {
         ISSL_REQUIRE(!(f & kWrongBucket), ISSL_ERR_FORMAT, where + "a site is listed under a bucket other than its key");
         bbase += nb;
     }
-    ix->srec.reserve(N);
-    k_site_records<<<grid_for(N), 256, 0, st>>>(ix->sigs.p, ix->occ.p, N, ix->srec.p);
-    ISSL_CUDA(cudaGetLastError());
     ISSL_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -359,6 +381,7 @@ void load_stream(issl_index* ix, Source& src, int device) {
 void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint32_t* d_occ, cudaStream_t st) {
     const uint64_t N = ix->n_sites, S = ix->n_slices;
     ISSL_REQUIRE(N < (1ull << 32), ISSL_ERR_UNSUPPORTED, "2^32 or more sites");
+    entry_packing(N, &ix->id_bits, &ix->occ_esc);
     ix->geom = make_geometry(ix->masks, ix->seq_len, N);
     ix->n_buckets = count_buckets(ix->geom);
     if (ix->sigs.p != d_sigs) {
@@ -371,7 +394,9 @@ void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint3
     }
     ix->d_geom.reserve(S);
     ISSL_CUDA(cudaMemcpyAsync(ix->d_geom.p, ix->geom.data(), S * sizeof(SliceGeom), cudaMemcpyHostToDevice, st));
-    ix->ids.reserve(S * N);
+    ix->entry_words = choose_entry_words(N, S, (bitsliced_words(ix->geom, N) + 4) * 4);
+    const uint64_t ew = ix->entry_words;
+    ix->ids.reserve(S * N * ew);
     ix->rbits.reserve(bitsliced_words(ix->geom, N) + 4);
     ix->offsets.reserve(ix->n_buckets + 1);
     DevBuf<uint32_t> keys, vals, keys2, vals2;
@@ -390,16 +415,14 @@ void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint3
         uint32_t *ko = keys.p, *vo = vals.p;
         // stable by key: ids stay ascending inside each bucket (ISSLCreateIndex.cpp:455-468)
         radix_sort_pairs_u32(keys.p, vals.p, keys2.p, vals2.p, N, 2 * g.width, temp.p, tb, st, &ko, &vo);
-        if (N) ISSL_CUDA(cudaMemcpyAsync(ix->ids.p + s * N, vo, N * 4, cudaMemcpyDeviceToDevice, st));
+        k_pack_entries<<<grid_for(N), 256, 0, st>>>(vo, ix->occ.p, N, ix->id_bits, ix->occ_esc, ix->entry_words,
+                                                    ix->ids.p + s * N * ew);
         k_offsets_from_sorted<<<grid_for(N + 1), 256, 0, st>>>(ko, N, nb, s * N, ix->offsets.p + bbase);
-        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(ix->ids.p + s * N, ix->sigs.p, N, g,
-                                                                    ix->rbits.p);
+        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(ix->ids.p + s * N * ew, ix->entry_words, ix->id_bits,
+                                                                    ix->sigs.p, N, g, ix->rbits.p);
         ISSL_CUDA(cudaGetLastError());
         bbase += nb;
     }
-    ix->srec.reserve(N);
-    k_site_records<<<grid_for(N), 256, 0, st>>>(ix->sigs.p, ix->occ.p, N, ix->srec.p);
-    ISSL_CUDA(cudaGetLastError());
     ISSL_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -408,7 +431,8 @@ void export_slice_lists(const issl_index* ix, uint64_t s, uint64_t* host_lists, 
     if (!N) return;
     DevBuf<uint64_t> tmp;
     tmp.reserve(N);
-    k_join_entries<<<grid_for(N), 256, 0, st>>>(ix->ids.p + s * N, ix->occ.p, N, tmp.p);
+    k_join_entries<<<grid_for(N), 256, 0, st>>>(ix->ids.p + s * N * ix->entry_words, ix->entry_words, ix->id_bits,
+                                                ix->occ.p, N, tmp.p);
     ISSL_CUDA(cudaGetLastError());
     ISSL_CUDA(cudaMemcpyAsync(host_lists, tmp.p, N * 8, cudaMemcpyDeviceToHost, st));
     ISSL_CUDA(cudaStreamSynchronize(st));
@@ -431,12 +455,14 @@ issl::IndexView issl_index::view() const {
     v.occ = occ.p;
     v.ids = ids.p;
     v.rbits = rbits.p;
-    v.srec = srec.p;
     v.offsets = offsets.p;
     v.geom = d_geom.p;
     v.n_sites = n_sites;
     v.n_slices = static_cast<uint32_t>(n_slices);
     v.n_buckets = static_cast<uint32_t>(n_buckets);
+    v.id_bits = id_bits;
+    v.occ_esc = occ_esc;
+    v.entry_words = entry_words;
     return v;
 }
 
@@ -536,8 +562,9 @@ int issl_index_get_info(const issl_index* ix, issl_index_info* out) {
         out->seq_len = ix->seq_len;
         out->n_slices = ix->n_slices;
         out->n_buckets = ix->n_buckets;
-        out->device_bytes = ix->sigs.bytes() + ix->occ.bytes() + ix->ids.bytes() + ix->rbits.bytes() + ix->srec.bytes() +
+        out->device_bytes = ix->sigs.bytes() + ix->occ.bytes() + ix->ids.bytes() + ix->rbits.bytes() +
                             ix->offsets.bytes() + ix->d_geom.bytes();
+        out->entry_bytes = static_cast<int>(4 * ix->entry_words);
         out->device = ix->device;
         int mn = 64, mx = 0;
         for (auto& g : ix->geom) {

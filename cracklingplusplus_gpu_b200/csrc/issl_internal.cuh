@@ -112,17 +112,24 @@ uint64_t bitsliced_words(const std::vector<SliceGeom>& geom, uint64_t n_sites);
 // ---- the resident index ------------------------------------------------------------------
 struct Workspace;
 
+// List entries are packed in 32 bits: the site id in the low id_bits bits, the occurrence count
+// in the bits above it when it is below occ_esc, else occ_esc ("look it up in occ[id]"). Up to
+// 2^29 sites the code has 3 bits, so a site with 1..6 occurrences (almost all of them) is scored
+// with one random read: this entry.
 struct IndexView {  // POD view handed to kernels
     const uint64_t* sigs;     // N packed signatures
     const uint32_t* occ;      // N occurrence counts (one per site)
-    const uint32_t* ids;      // S*N site ids in list order (slice-major)
+    const uint32_t* ids;      // S*N list entries in list order (slice-major), entry_words words each:
+                              // the packed id, then (entry_words 2) the residual code
     const uint32_t* rbits;    // bit-sliced residual codes (see SliceGeom)
-    const uint4* srec;        // N site records (signature low, signature high, occurrences, 0)
     const uint64_t* offsets;  // G+1 bucket starts in global entry numbering: s*N + position
     const SliceGeom* geom;    // S slice descriptors
     uint64_t n_sites;
     uint32_t n_slices;
     uint32_t n_buckets;       // sum of 4^w
+    uint32_t id_bits;         // bits of the site id in a packed entry (1..32)
+    uint32_t occ_esc;         // occurrence codes >= occ_esc mean "read occ[id]" (0: always)
+    uint32_t entry_words;     // 2: entries carry the residual code; 1: packed id only
 };
 
 }  // namespace issl
@@ -135,12 +142,13 @@ struct issl_index {
     issl::DevBuf<uint64_t> sigs;
     issl::DevBuf<uint32_t> occ, ids, rbits;
     issl::DevBuf<uint64_t> offsets;  // n_buckets + 1 global bucket starts
-    issl::DevBuf<uint4> srec;        // per site: signature and occurrences in one 16-byte record
+    uint32_t id_bits = 32, occ_esc = 0;  // packing of the list entries (IndexView)
+    uint32_t entry_words = 2;            // 32-bit words per list entry (IndexView)
     issl::DevBuf<issl::SliceGeom> d_geom;
     std::unique_ptr<issl::Workspace> ws;
     issl_score_stats stats{};
-    // scan unit size per bucket-size class, staging depth, blocks per SM (issl_set_tuning)
-    issl_tuning tuning{{1024, 1024, 1024}, 3, 0};
+    // scan unit size per bucket-size class, staging depth, blocks per SM, first slice wave
+    issl_tuning tuning{{1024, 1024, 1024}, 3, 0, 1};
     uint32_t tuning_version = 0;
     issl::IndexView view() const;
     issl_index();  // defined where Workspace is complete
@@ -148,6 +156,31 @@ struct issl_index {
 };
 
 namespace issl {
+
+// entry packing for an index of n sites: 29 id bits and a 3-bit occurrence code (counts 0..6
+// stored, 7 = escape) up to 2^29 sites; beyond that the id takes the bits it needs and the code
+// what is left (no code at 2^31 sites and more: every count is read from occ[id])
+inline void entry_packing(uint64_t n, uint32_t* id_bits, uint32_t* occ_esc) {
+    uint32_t b = 29;
+    while (b < 32 && (1ull << b) < n) b++;
+    *id_bits = b;
+    *occ_esc = b < 32 ? (1u << (32 - b)) - 1u : 0u;
+}
+__host__ __device__ __forceinline__ uint32_t pack_entry(uint32_t id, uint32_t occ, uint32_t id_bits, uint32_t occ_esc) {
+    return id_bits < 32 ? id | ((occ < occ_esc ? occ : occ_esc) << id_bits) : id;
+}
+__host__ __device__ __forceinline__ uint32_t entry_id(uint32_t e, uint32_t id_bits) {
+    return id_bits < 32 ? e & ((1u << id_bits) - 1u) : e;
+}
+// occurrence count of a packed entry (one more read only for escaped counts)
+__device__ __forceinline__ uint32_t entry_occ(uint32_t e, const IndexView& v) {
+    const uint32_t c = v.id_bits < 32 ? e >> v.id_bits : 0u;
+    return c < v.occ_esc ? c : v.occ[entry_id(e, v.id_bits)];
+}
+
+// 8-byte list entries (id + residual code) when the index leaves room for them beside the scoring
+// workspaces, else 4-byte entries; ISSL_ENTRY_BYTES=4 or 8 forces a width (index.cu)
+uint32_t choose_entry_words(uint64_t n_sites, uint64_t n_slices, uint64_t rbits_bytes);
 
 // builders (index.cu)
 void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint32_t* d_occ,

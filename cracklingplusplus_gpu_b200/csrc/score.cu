@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -51,21 +52,27 @@ struct UnitDesc {   // 16 bytes
 };
 
 struct Counters {
+    // per wave (cleared at the start of every wave: the fields before `overflow`)
     uint64_t bucket_total;  // hi: units, lo: probes into non-empty buckets
     uint32_t n_units;       // min(units, capacity)
     uint32_t n_cand;        // hit slots reserved by the scan (may exceed capacity -> overflow)
     uint32_t hit_total;     // owned hits: sum of per-guide hits (scan total)
     uint32_t n_big;         // exiting guides with more than kWarpSort hits (block scorer)
     uint32_t n_exit;        // exiting guides with at most kWarpSort hits (warp scorer)
-    uint32_t overflow;      // 1: units, 2: hits, 4: a bounded wait in the scan gave up
     uint32_t next_batch;    // work queue of the scan: next batch of 32 units to take
+    // per call
+    uint32_t overflow;      // 1: units, 2: hits, 4: a bounded wait in the scan gave up
+    uint32_t act_n[2];      // guides still scoring after a wave (active lists A and B)
     uint32_t pad;
+    uint64_t max_units, max_cand;        // largest wave (to size the buffers)
+    uint64_t probes, units, hits, cands; // summed over the waves
     uint64_t distinct;
     uint64_t buckets;       // distinct buckets probed
     uint64_t entries;       // entries compared by the scan (per guide group)
     uint64_t rbytes;        // bit-sliced bytes the scan copies
     uint64_t class_probes[3];  // probes into buckets of < 64, 64..4095, >= 4096 entries
 };
+constexpr size_t kWaveCounterBytes = offsetof(Counters, overflow);
 
 struct Tables {  // device copies of the penalty tables
     double mit[6195];
@@ -147,7 +154,7 @@ __host__ __device__ inline WarpLayout warp_layout(uint32_t max_wpb, uint32_t sta
 struct issl::Workspace {
     int device = 0;
     cudaStream_t own_stream = nullptr;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev[2 + 2 * 2] = {};  // call start / end, then scan start / end of each slice wave
     size_t q_cap = 0, unit_cap = 0, cand_cap = 0;
     uint64_t g_cap = 0;
     int scan_blocks = 0;
@@ -180,6 +187,8 @@ struct issl::Workspace {
     // batch form: set table (header + sets) on the device and its pinned host staging, the
     // guide -> set map, and the captured pipeline
     DevBuf<uint16_t> qset;
+    DevBuf<uint32_t> active[2];  // guides still scoring after a slice wave (double-buffered)
+    DevBuf<uint64_t> acc;        // their running totals (5 words per guide)
     DevBuf<uint8_t> batch;
     uint8_t* h_batch = nullptr;
     size_t sets_cap = 0;
@@ -224,17 +233,34 @@ __global__ void k_encode_ascii(const char* __restrict__ ascii, size_t stride, ui
 // n: guides, or *d_n when the count lives on the device (batch form)
 __device__ __forceinline__ uint64_t guide_count(const uint32_t* d_n, uint64_t n) { return d_n ? *d_n : n; }
 
-__global__ void k_probe_count(IndexView ix, const uint64_t* __restrict__ qsig, const uint32_t* d_n, uint64_t n,
+// The probes of one wave: every guide still scoring x the wave's slices [s0, s0 + sw). Guides
+// are the list `active` of *d_nact entries, or all guides (active == nullptr) in the first wave.
+struct WaveProbes {
+    const uint32_t* active;
+    const uint32_t* d_nact;
+    const uint32_t* d_n;
+    uint64_t n;
+    uint32_t s0, sw;
+    __device__ uint64_t guides() const { return d_nact ? *d_nact : guide_count(d_n, n); }
+    __device__ void at(uint64_t p, uint64_t& q, uint32_t& s) const {
+        const uint64_t i = p / sw;
+        s = s0 + static_cast<uint32_t>(p - i * sw);
+        q = active ? active[i] : i;
+    }
+};
+
+__global__ void k_probe_count(IndexView ix, const uint64_t* __restrict__ qsig, WaveProbes wp,
                               uint32_t* __restrict__ probe_gb, uint32_t* __restrict__ bucket_cnt,
                               const uint64_t* __restrict__ off) {
     __shared__ SliceGeom g[kMaxSlices];
     for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
     __syncthreads();
-    const uint64_t S = ix.n_slices, total = guide_count(d_n, n) * S;
+    const uint64_t total = wp.guides() * wp.sw;
     for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < total;
          p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t q = p / S;
-        const uint32_t s = static_cast<uint32_t>(p - q * S);
+        uint64_t q;
+        uint32_t s;
+        wp.at(p, q, s);
         const uint32_t gb = g[s].bbase + slice_key(qsig[q], g[s]);
         const bool nonempty = off[gb + 1] > off[gb];
         probe_gb[p] = nonempty ? gb : kEmpty;
@@ -243,12 +269,15 @@ __global__ void k_probe_count(IndexView ix, const uint64_t* __restrict__ qsig, c
 }
 
 // 2. bucket scan: value = (units << 32) | probes
+// g counts from g0, the first bucket of the wave's slices
 struct BucketLoad {
     const uint32_t* cnt;
     const uint64_t* off;
     uint64_t n_sites;
     ChunkClasses cc;
-    __device__ uint64_t operator()(uint64_t g) const {
+    uint64_t g0;
+    __device__ uint64_t operator()(uint64_t gi) const {
+        const uint64_t g = g0 + gi;
         const uint32_t c = cnt[g];
         if (!c) return 0;
         // chunks are aligned to the chunk size within the slice (which divides kChunk), so a
@@ -269,7 +298,9 @@ struct BucketStore {
     uint64_t unit_cap;
     uint64_t n_sites;
     ChunkClasses cc;
-    __device__ void operator()(uint64_t g, uint64_t ex, uint64_t inc) const {
+    uint64_t g0;
+    __device__ void operator()(uint64_t gi, uint64_t ex, uint64_t inc) const {
+        const uint64_t g = g0 + gi;
         qstart[g] = static_cast<uint32_t>(ex);
         const uint32_t c = static_cast<uint32_t>(inc) - static_cast<uint32_t>(ex);
         if (!c) return;
@@ -300,10 +331,10 @@ struct BucketStore {
 
 // work counters for the roofline: distinct buckets scanned and entries streamed (a bucket's
 // entries are read once per group of up to kGroup guides)
-__global__ void k_bucket_stats(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off, uint64_t G,
-                               const SliceGeom* __restrict__ geom, uint64_t n_sites, Counters* c) {
+__global__ void k_bucket_stats(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off, uint64_t g0,
+                               uint64_t g1, const SliceGeom* __restrict__ geom, uint64_t n_sites, Counters* c) {
     uint64_t buckets = 0, entries = 0, bytes = 0, cp[3] = {0, 0, 0};
-    for (uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < G;
+    for (uint64_t g = g0 + blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < g1;
          g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint32_t k = cnt[g];
         if (!k) continue;
@@ -334,22 +365,26 @@ __global__ void k_units_finalize(Counters* c, uint64_t unit_cap) {
     const uint64_t u = c->bucket_total >> 32;
     c->n_units = static_cast<uint32_t>(u < unit_cap ? u : unit_cap);
     if (u > unit_cap) atomicOr(&c->overflow, 1u);
+    if (u > c->max_units) c->max_units = u;
+    c->units += u;
+    c->probes += c->bucket_total & 0xFFFFFFFFull;
 }
 
 // 3. guides grouped by bucket; each slot holds (guide index, guide residual code for the slice)
-__global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig, const uint32_t* d_n, uint64_t n,
+__global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig, WaveProbes wp,
                                 const uint32_t* __restrict__ probe_gb, uint32_t* __restrict__ bucket_cnt,
                                 const uint32_t* __restrict__ qstart, uint64_t* __restrict__ probe_qr) {
     __shared__ SliceGeom g[kMaxSlices];
     for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
     __syncthreads();
-    const uint64_t S = ix.n_slices, total = guide_count(d_n, n) * S;
+    const uint64_t total = wp.guides() * wp.sw;
     for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < total;
          p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint32_t gb = probe_gb[p];
         if (gb == kEmpty) continue;
-        const uint64_t q = p / S;
-        const uint32_t s = static_cast<uint32_t>(p - q * S);
+        uint64_t q;
+        uint32_t s;
+        wp.at(p, q, s);
         // the decrement leaves bucket_cnt all zero for the next call
         const uint32_t slot = qstart[gb] + atomicSub(&bucket_cnt[gb], 1u) - 1u;
         probe_qr[slot] = q | (static_cast<uint64_t>(slice_residual(qsig[q], g[s])) << 32);
@@ -604,6 +639,8 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
 
 __global__ void k_cands_finalize(Counters* c, uint32_t cand_cap) {
     if (c->n_cand > cand_cap) atomicOr(&c->overflow, 2u);
+    if (c->n_cand > c->max_cand) c->max_cand = c->n_cand;
+    c->cands += c->n_cand;
 }
 
 // 5. the ownership rule on the candidates: a site reached in slice s is counted only if no
@@ -666,12 +703,17 @@ struct StoreQoff {
     }
 };
 
-// One thread per owned hit (many independent loads in flight): the site id, then the site record
-// (signature, occurrences), written into the guide's segment so that the scorers read only
-// contiguous data.
-__global__ void k_hit_scatter(const uint4* __restrict__ cands, const Counters* c, uint32_t* __restrict__ qhits,
-                              const uint32_t* __restrict__ qhoff, IndexView ix, uint4* __restrict__ seg,
-                              uint64_t* __restrict__ segsig) {
+// One thread per owned hit (many independent loads in flight): the list entry gives the site id,
+// its occurrences and (8-byte entries) its residual code, from which the signature is rebuilt;
+// with 4-byte entries the signature is a second read. Written into the guide's segment so that
+// the scorers read only contiguous data.
+__global__ void k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint32_t* __restrict__ qhits,
+                              const uint32_t* __restrict__ qhoff, IndexView ix, const uint64_t* __restrict__ qsig,
+                              uint4* __restrict__ seg, uint64_t* __restrict__ segsig) {
+    __shared__ SliceGeom g[kMaxSlices];
+    for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) c->hits += c->hit_total;
     if (c->overflow) return;
     const uint32_t n = c->n_cand;
     for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x) {
@@ -679,13 +721,14 @@ __global__ void k_hit_scatter(const uint4* __restrict__ cands, const Counters* c
         if (r.x == kDeadCand) continue;
         const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
         const uint32_t sl = r.x >> kGuideBits;
-        const uint32_t id = ix.ids[static_cast<uint64_t>(sl) * ix.n_sites + r.y];
-        const uint4 sr = ix.srec[id];
+        uint32_t id, occ;
+        uint64_t sig;
+        load_site(ix, sl, r.y, qsig[q], g[sl], id, occ, sig);
         // the decrement leaves qhits all zero for the next call
         const uint32_t slot = qhoff[q] + atomicSub(&qhits[q], 1u) - 1u;
         // seg record: (list position, slice, site id, occurrences) + the site signature
-        seg[slot] = make_uint4(r.y, sl, id, sr.z);
-        segsig[slot] = (static_cast<uint64_t>(sr.y) << 32) | sr.x;
+        seg[slot] = make_uint4(r.y, sl, id, occ);
+        segsig[slot] = sig;
     }
 }
 
@@ -785,6 +828,8 @@ __device__ __forceinline__ uint64_t warp_incl_sum_u64(uint64_t v, int lane) {
     return v;
 }
 
+struct Acc;
+
 struct ScoreArgs {
     IndexView ix;
     const uint64_t* qsig;
@@ -805,6 +850,14 @@ struct ScoreArgs {
     double* out_cfd;
     char* out_code;
     uint64_t* out_count;
+    // slice waves: the guides of this wave, the guides that go on to the next one, and the
+    // running totals carried between waves
+    const uint32_t* active;  // nullptr: every guide (first wave)
+    const uint32_t* d_nact;
+    uint32_t* next_active;
+    uint32_t* d_nnext;
+    Acc* acc;
+    int first_wave, last_wave;
 };
 
 __device__ __forceinline__ ScoreParams params_of(const ScoreArgs& a, uint64_t qi) {
@@ -858,6 +911,12 @@ struct FxContribution {
     uint64_t occ;
 };
 
+// running totals of a guide carried from one slice wave to the next
+struct Acc {
+    Fx mit, cfd;
+    uint64_t occ;
+};
+
 // r: seg record (position, slice, site id, occurrences), sig: the site's signature
 __device__ __forceinline__ FxContribution fx_contribution(const ScoreParams& P, const Tables& T, uint64_t q,
                                                          const uint4& r, uint64_t sig) {
@@ -876,8 +935,9 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
     const Tables& T = *a.tables;
     if (a.counters->overflow) return;  // rerun follows
     const uint64_t gw = blockIdx.x * 8ull + warp, nw = gridDim.x * 8ull;
-    const uint64_t n = guide_count(a.d_n, a.n);
-    for (uint64_t qi = gw; qi < n; qi += nw) {
+    const uint64_t n = a.d_nact ? *a.d_nact : guide_count(a.d_n, a.n);
+    for (uint64_t i = gw; i < n; i += nw) {
+        const uint64_t qi = a.active ? a.active[i] : i;
         const ScoreParams P = params_of(a, qi);
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         const uint64_t q = a.qsig[qi];
@@ -885,8 +945,8 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         const uint64_t* sig = a.segsig + h0;
         Fx tm{0, 0}, tc{0, 0};
         uint64_t tn = 0;
-        for (uint32_t i = lane; i < L; i += 32) {
-            const FxContribution c = fx_contribution(P, T, q, seg[i], sig[i]);
+        for (uint32_t j = lane; j < L; j += 32) {
+            const FxContribution c = fx_contribution(P, T, q, seg[j], sig[j]);
             tm = fx_add(tm, c.mit);
             tc = fx_add(tc, c.cfd);
             tn += c.occ;
@@ -894,6 +954,12 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         tm = fx_warp_sum(tm);
         tc = fx_warp_sum(tc);
         for (int d = 16; d > 0; d >>= 1) tn += __shfl_xor_sync(0xffffffffu, tn, d);
+        if (!a.first_wave) {
+            const Acc pr = a.acc[qi];
+            tm = fx_add(tm, pr.mit);
+            tc = fx_add(tc, pr.cfd);
+            tn += pr.occ;
+        }
         if (exit_test(P, fx_double(tm), fx_double(tc))) {
             if (lane == 0) {
                 if (L <= static_cast<uint32_t>(kWarpSort))
@@ -904,12 +970,18 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
             continue;
         }
         if (P.want_distinct)
-            for (uint32_t i = lane; i < L; i += 32) {
-                const uint32_t id = seg[i].z;
+            for (uint32_t j = lane; j < L; j += 32) {
+                const uint32_t id = seg[j].z;
                 atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
-        if (lane == 0)
-            finalise(P, fx_double(tm), fx_double(tc), tn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+        if (lane == 0) {
+            if (a.last_wave) {
+                finalise(P, fx_double(tm), fx_double(tc), tn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+            } else {
+                a.acc[qi] = Acc{tm, tc, tn};
+                a.next_active[atomicAdd(a.d_nnext, 1u)] = static_cast<uint32_t>(qi);
+            }
+        }
     }
 }
 
@@ -938,6 +1010,14 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
     for (uint32_t e = gw; e < n_exit; e += nw) {
         const uint64_t qi = a.exitq[e];
         const ScoreParams P = params_of(a, qi);
+        Fx rm{0, 0}, rc{0, 0};  // totals of the earlier waves
+        uint64_t rn = 0;
+        if (!a.first_wave) {
+            const Acc pr = a.acc[qi];
+            rm = pr.mit;
+            rc = pr.cfd;
+            rn = pr.occ;
+        }
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         const uint64_t q = a.qsig[qi];
         const uint4* seg = a.seg + h0;
@@ -960,8 +1040,6 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
         __syncwarp();
         for (uint32_t i = lane; i < L; i += 32) W.idx[atomicAdd(&W.cur[seg[i].y], 1u)] = static_cast<uint16_t>(i);
         __syncwarp();
-        Fx rm{0, 0}, rc{0, 0};
-        uint64_t rn = 0;
         bool stopped = false;
         for (uint32_t sl = 0; sl < S && !stopped; sl++) {
             const uint32_t b0 = W.cnt[sl], ns = W.cnt[sl + 1] - b0;
@@ -1058,6 +1136,14 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
     for (uint32_t b = blockIdx.x; b < n_big; b += gridDim.x) {
         const uint64_t qi = a.big[b];
         const ScoreParams P = params_of(a, qi);
+        Fx run_m{0, 0}, run_c{0, 0};  // totals of the earlier waves
+        uint64_t run_n = 0;
+        if (!a.first_wave) {
+            const Acc pr = a.acc[qi];
+            run_m = pr.mit;
+            run_c = pr.cfd;
+            run_n = pr.occ;
+        }
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         uint4* seg = a.seg + h0;
         uint64_t* sig = a.segsig + h0;
@@ -1095,8 +1181,6 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
                 __syncthreads();
             }
         }
-        Fx run_m{0, 0}, run_c{0, 0};
-        uint64_t run_n = 0;
         bool stopped = false;
         for (uint32_t c0 = 0; c0 < L && !stopped; c0 += blockDim.x) {
             const uint32_t t = c0 + threadIdx.x;
@@ -1252,7 +1336,28 @@ void apply_tuning(issl_index* ix, Workspace& ws) {
     ws.tuning_version = ix->tuning_version;
 }
 
+// A failed allocation leaves some buffers released: forget every capacity so that the next call
+// reallocates what is missing (and re-zeroes the counters that must start at zero).
+template <class F>
+void with_alloc_guard(Workspace& ws, F&& f) {
+    try {
+        f();
+    } catch (...) {
+        ws.q_cap = ws.unit_cap = ws.cand_cap = 0;
+        ws.g_cap = 0;
+        ws.zero_state_ok = false;
+        ws.epoch++;
+        throw;
+    }
+}
+
+void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st);
+
 void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st) {
+    with_alloc_guard(ws, [&] { ensure_capacity_impl(ix, ws, n, batch, st); });
+}
+
+void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st) {
     const uint64_t S = ix->n_slices, G = ix->n_buckets;
     apply_tuning(ix, ws);
     if (ws.g_cap < G + 1) {
@@ -1276,6 +1381,9 @@ void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaSt
         ws.out_code.reserve(cap);
         ws.out_count.reserve(cap);
         ws.out_distinct.reserve(1);
+        ws.active[0].reserve(cap);
+        ws.active[1].reserve(cap);
+        ws.acc.reserve(cap * 5);
         if (ws.qset.p) ws.qset.reserve(cap);
         ISSL_CUDA(cudaMemsetAsync(ws.qhits.p, 0, (cap + 1) * 4, st));
         ws.q_cap = cap;
@@ -1324,8 +1432,10 @@ void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide,
     *per_candidate = sizeof(uint4) * 2 + sizeof(uint64_t);
     *fixed = 8 * (G + 1) + sizeof(Tables) + sizeof(Counters) + (kScanBlocks + 4) * 12 + 4096 * sizeof(UnitDesc) +
              (65536 + slab_slack) * *per_candidate;
-    // qsig, probe lists, hit counts and offsets, exit queues, outputs, set map; scan units
-    *per_guide = 8 + 12 * S + 4 * 4 + (8 + 8 + 1 + 8) + 2 + sizeof(UnitDesc) * 3 * S * (kChunk / min_chunk);
+    // qsig, probe lists, hit counts and offsets, exit queues, outputs, set map, wave lists and
+    // running totals; scan units
+    *per_guide = 8 + 12 * S + 4 * 4 + (8 + 8 + 1 + 8) + 2 + 2 * 4 + 5 * 8 +
+                 sizeof(UnitDesc) * 3 * S * (kChunk / min_chunk);
 }
 
 namespace {
@@ -1368,6 +1478,9 @@ struct RunSpec {
     char* code = nullptr;
     uint64_t* count = nullptr;
     bool events = true;  // record the timing events (not inside a graph capture)
+    // distinct-site count over several runs (guide chunks): clear the bitmap in the first, count
+    // it in the last
+    bool distinct_first = true, distinct_last = true;
 };
 
 __global__ void k_expand_sets(const BatchHeader* __restrict__ hdr, const SetDesc* __restrict__ sets,
@@ -1384,6 +1497,16 @@ __global__ void k_expand_sets(const BatchHeader* __restrict__ hdr, const SetDesc
     }
 }
 
+// Slice waves of a call: the first `first_wave` slices, then the rest (one wave when first_wave
+// is 0 or covers every slice). The reference visits slices in order and stops a guide at the hit
+// where its test fires; a guide whose test fires within the first wave never probes the later
+// slices, which bounds the work and memory of guides with thousands of hits.
+std::vector<std::pair<uint32_t, uint32_t>> slice_waves(const issl_index* ix) {
+    const uint32_t S = static_cast<uint32_t>(ix->n_slices), fw = ix->tuning.first_wave;
+    if (fw > 0 && fw < S) return {{0u, fw}, {fw, S}};
+    return {{0u, S}};
+}
+
 // Enqueues the whole pipeline. Returns the number of kernels it launched.
 uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaStream_t st) {
     const IndexView v = ix->view();
@@ -1394,83 +1517,100 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
     const int sms = sm_count(ix->device);
     const issl_tuning& tn = ix->tuning;
     const ChunkClasses cc{{tn.chunk[0], tn.chunk[1], tn.chunk[2]}};
+    Counters* C = ws.counters.p;
     uint64_t k = 0;
-    ISSL_CUDA(cudaMemsetAsync(ws.counters.p, 0, sizeof(Counters), st));
+    ISSL_CUDA(cudaMemsetAsync(C, 0, sizeof(Counters), st));
     const uint64_t* off = ix->offsets.p;
     if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[0], st));
     if (batch) {
         k_expand_sets<<<grid_for(n, 256, sms * 8), 256, 0, st>>>(R.hdr, R.sets, ws.qset.p);
         k++;
     }
-    k_probe_count<<<grid_for(n * S, 256, sms * 16), 256, 0, st>>>(v, R.qsig, d_n, n, ws.probe_gb.p, ws.bucket_cnt.p,
-                                                                   off);
-    device_scan<uint64_t, OpSum>(BucketLoad{ws.bucket_cnt.p, off, ix->n_sites, cc},
-                                 BucketStore{ws.bucket_cnt.p, off, ws.bucket_qstart.p, ws.units.p, ws.unit_cap,
-                                             ix->n_sites, cc},
-                                 nullptr, G, ws.scan64.p, &ws.counters.p->bucket_total, st);
-    k_units_finalize<<<1, 1, 0, st>>>(ws.counters.p, ws.unit_cap);
-    k_bucket_stats<<<sms * 4, 256, 0, st>>>(ws.bucket_cnt.p, off, G, ix->d_geom.p, ix->n_sites, ws.counters.p);
-    k_probe_scatter<<<grid_for(n * S, 256, sms * 16), 256, 0, st>>>(v, R.qsig, d_n, n, ws.probe_gb.p,
-                                                                     ws.bucket_cnt.p, ws.bucket_qstart.p,
-                                                                     ws.probe_qr.p);
-    k += 7;
-    ScanArgs sa;
-    sa.rbits = ix->rbits.p;
-    sa.geom = ix->d_geom.p;
-    sa.units = ws.units.p;
-    sa.probe_qr = ws.probe_qr.p;
-    sa.counters = ws.counters.p;
-    sa.cands = ws.cands.p;
-    sa.n_slices = static_cast<uint32_t>(S);
-    sa.cand_cap = static_cast<uint32_t>(std::min<size_t>(ws.cand_cap, 0xFFFFFFFFull));
-    sa.max_dist = R.P.max_dist;
-    sa.hdr = R.hdr;
-    sa.L = ws.scan_layout;
-    if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[1], st));
-    switch (ws.scan_rw) {
-        case 12: k_scan<12><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
-        case 10: k_scan<10><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
-        case 16: k_scan<16><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
-        default: k_scan<0><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
+    if (R.P.want_distinct && R.distinct_first)
+        ISSL_CUDA(cudaMemsetAsync(ws.bitmap.p, 0, (ix->n_sites / 32 + 1) * 4, st));
+    const auto waves = slice_waves(ix);
+    for (size_t w = 0; w < waves.size(); w++) {
+        const bool first = w == 0, last = w + 1 == waves.size();
+        const uint32_t s0 = waves[w].first, s1 = waves[w].second, cur = w & 1u, nxt = cur ^ 1u;
+        if (!first) ISSL_CUDA(cudaMemsetAsync(C, 0, kWaveCounterBytes, st));
+        if (!last) ISSL_CUDA(cudaMemsetAsync(&C->act_n[nxt], 0, 4, st));
+        const WaveProbes wp{first ? nullptr : ws.active[cur].p, first ? nullptr : &C->act_n[cur], d_n, n, s0, s1 - s0};
+        const uint64_t g0 = ix->geom[s0].bbase, g1 = s1 < S ? ix->geom[s1].bbase : G;
+        const unsigned pgrid = grid_for(n * (s1 - s0), 256, sms * 16);
+        k_probe_count<<<pgrid, 256, 0, st>>>(v, R.qsig, wp, ws.probe_gb.p, ws.bucket_cnt.p, off);
+        device_scan<uint64_t, OpSum>(BucketLoad{ws.bucket_cnt.p, off, ix->n_sites, cc, g0},
+                                     BucketStore{ws.bucket_cnt.p, off, ws.bucket_qstart.p, ws.units.p, ws.unit_cap,
+                                                 ix->n_sites, cc, g0},
+                                     nullptr, g1 - g0, ws.scan64.p, &C->bucket_total, st);
+        k_units_finalize<<<1, 1, 0, st>>>(C, ws.unit_cap);
+        k_bucket_stats<<<sms * 4, 256, 0, st>>>(ws.bucket_cnt.p, off, g0, g1, ix->d_geom.p, ix->n_sites, C);
+        k_probe_scatter<<<pgrid, 256, 0, st>>>(v, R.qsig, wp, ws.probe_gb.p, ws.bucket_cnt.p, ws.bucket_qstart.p,
+                                               ws.probe_qr.p);
+        k += 7;
+        ScanArgs sa;
+        sa.rbits = ix->rbits.p;
+        sa.geom = ix->d_geom.p;
+        sa.units = ws.units.p;
+        sa.probe_qr = ws.probe_qr.p;
+        sa.counters = C;
+        sa.cands = ws.cands.p;
+        sa.n_slices = static_cast<uint32_t>(S);
+        sa.cand_cap = static_cast<uint32_t>(std::min<size_t>(ws.cand_cap, 0xFFFFFFFFull));
+        sa.max_dist = R.P.max_dist;
+        sa.hdr = R.hdr;
+        sa.L = ws.scan_layout;
+        if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[2 + 2 * w], st));
+        switch (ws.scan_rw) {
+            case 12: k_scan<12><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
+            case 10: k_scan<10><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
+            case 16: k_scan<16><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
+            default: k_scan<0><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
+        }
+        if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[3 + 2 * w], st));
+        k_cands_finalize<<<1, 1, 0, st>>>(C, sa.cand_cap);
+        k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, v, ws.qhits.p, R.sets, qset);
+        device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, d_n, n, ws.scan32.p, &C->hit_total,
+                                     st);
+        k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, ws.qhits.p, ws.qhoff.p, v, R.qsig, ws.seg.p,
+                                               ws.segsig.p);
+        k += 7;
+        ScoreArgs a;
+        a.ix = v;
+        a.qsig = R.qsig;
+        a.seg = ws.seg.p;
+        a.segsig = ws.segsig.p;
+        a.exitq = ws.exitq.p;
+        a.qhoff = ws.qhoff.p;
+        a.tables = ws.tables.p;
+        a.counters = C;
+        a.big = ws.big.p;
+        a.bitmap = ws.bitmap.p;
+        a.n = n;
+        a.d_n = d_n;
+        a.P = R.P;
+        a.sets = R.sets;
+        a.qset = qset;
+        a.out_mit = R.mit;
+        a.out_cfd = R.cfd;
+        a.out_code = R.code;
+        a.out_count = R.count;
+        a.active = wp.active;
+        a.d_nact = wp.d_nact;
+        a.next_active = ws.active[nxt].p;
+        a.d_nnext = &C->act_n[nxt];
+        a.acc = reinterpret_cast<Acc*>(ws.acc.p);
+        a.first_wave = first;
+        a.last_wave = last;
+        k_score_sum<<<grid_for(n, 8, sms * 8), 256, 0, st>>>(a);
+        k_score_ordered<<<sms * 4, 256, 8 * sizeof(OrderedSmem), st>>>(a);
+        k_score_block<<<sms * 2, 256, kBlockHits * sizeof(uint64_t), st>>>(a);
+        k += 3;
     }
-    if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[2], st));
-    k_cands_finalize<<<1, 1, 0, st>>>(ws.counters.p, sa.cand_cap);
-    k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, v, ws.qhits.p, R.sets, qset);
-    device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, d_n, n, ws.scan32.p,
-                                 &ws.counters.p->hit_total, st);
-    k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, ws.counters.p, ws.qhits.p, ws.qhoff.p, v, ws.seg.p,
-                                           ws.segsig.p);
-    k += 7;
-    if (R.P.want_distinct) ISSL_CUDA(cudaMemsetAsync(ws.bitmap.p, 0, (ix->n_sites / 32 + 1) * 4, st));
-    ScoreArgs a;
-    a.ix = v;
-    a.qsig = R.qsig;
-    a.seg = ws.seg.p;
-    a.segsig = ws.segsig.p;
-    a.exitq = ws.exitq.p;
-    a.qhoff = ws.qhoff.p;
-    a.tables = ws.tables.p;
-    a.counters = ws.counters.p;
-    a.big = ws.big.p;
-    a.bitmap = ws.bitmap.p;
-    a.n = n;
-    a.d_n = d_n;
-    a.P = R.P;
-    a.sets = R.sets;
-    a.qset = qset;
-    a.out_mit = R.mit;
-    a.out_cfd = R.cfd;
-    a.out_code = R.code;
-    a.out_count = R.count;
-    k_score_sum<<<grid_for(n, 8, sms * 8), 256, 0, st>>>(a);
-    k_score_ordered<<<sms * 4, 256, 8 * sizeof(OrderedSmem), st>>>(a);
-    k_score_block<<<sms * 2, 256, kBlockHits * sizeof(uint64_t), st>>>(a);
-    k += 3;
-    if (R.P.want_distinct) {
-        k_popcount<<<sms * 4, 256, 0, st>>>(ws.bitmap.p, ix->n_sites / 32 + 1, ws.counters.p);
+    if (R.P.want_distinct && R.distinct_last) {
+        k_popcount<<<sms * 4, 256, 0, st>>>(ws.bitmap.p, ix->n_sites / 32 + 1, C);
         k++;
     }
-    if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[3], st));
+    if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[1], st));
     ISSL_CUDA(cudaGetLastError());
     return k;
 }
@@ -1485,23 +1625,25 @@ bool check_and_grow(Workspace& ws, cudaStream_t st) {
         ws.zero_state_ok = false;
         throw Error(ISSL_ERR_TIMEOUT, "scan: an asynchronous copy did not complete within the wait limit");
     }
-    const uint64_t units = c.bucket_total >> 32;
+    const uint64_t units = c.max_units;
     bool ok = true;
-    if (units > ws.unit_cap) {
-        ws.units.reserve(units + units / 8 + 1024);
-        ws.unit_cap = units + units / 8 + 1024;
-        ok = false;
-    }
-    if (c.n_cand > ws.cand_cap || (c.overflow & 2u)) {
-        const size_t cap = static_cast<size_t>(c.n_cand) + c.n_cand / 4 + 65536;
-        ISSL_REQUIRE(cap < 0xFFFFFFFFull, ISSL_ERR_UNSUPPORTED,
-                     "more than 2^32 candidate sites in one call; split the guides");
-        ws.cands.reserve(cap);
-        ws.seg.reserve(cap);
-        ws.segsig.reserve(cap);
-        ws.cand_cap = cap;
-        ok = false;
-    }
+    with_alloc_guard(ws, [&] {
+        if (units > ws.unit_cap) {
+            ws.units.reserve(units + units / 8 + 1024);
+            ws.unit_cap = units + units / 8 + 1024;
+            ok = false;
+        }
+        if (c.max_cand > ws.cand_cap || (c.overflow & 2u)) {
+            const size_t cap = static_cast<size_t>(c.max_cand) + c.max_cand / 4 + 65536;
+            ISSL_REQUIRE(cap < 0xFFFFFFFFull, ISSL_ERR_UNSUPPORTED,
+                         "more than 2^32 candidate sites in one slice wave; split the guides");
+            ws.cands.reserve(cap);
+            ws.seg.reserve(cap);
+            ws.segsig.reserve(cap);
+            ws.cand_cap = cap;
+            ok = false;
+        }
+    });
     if (!ok) {
         ws.zero_state_ok = false;  // counters of the aborted run are not drained
         ws.epoch++;
@@ -1512,52 +1654,103 @@ bool check_and_grow(Workspace& ws, cudaStream_t st) {
 void fill_stats(const Workspace& ws, float scan_ms, float total_ms, uint64_t launches, issl_score_stats& s) {
     s.scan_ms = scan_ms;
     s.total_ms = total_ms;
-    s.probes = static_cast<uint64_t>(ws.last.bucket_total & 0xFFFFFFFFull);
-    s.units = ws.last.bucket_total >> 32;
-    s.hits = ws.last.hit_total;
+    s.probes = ws.last.probes;
+    s.units = ws.last.units;
+    s.hits = ws.last.hits;
     s.buckets_scanned = ws.last.buckets;
     s.entries_scanned = ws.last.entries;
     // bytes the scan must move: the bit-sliced blocks it copies, 16 per unit descriptor, 8 per
     // guide of a unit (index + residual), 16 per candidate slot written
-    s.scan_bytes = ws.last.rbytes + 16 * s.units + 8 * s.probes + 16 * static_cast<uint64_t>(ws.last.n_cand);
+    s.scan_bytes = ws.last.rbytes + 16 * s.units + 8 * s.probes + 16 * ws.last.cands;
     s.launches = launches;
     for (int i = 0; i < 3; i++) s.class_probes[i] = ws.last.class_probes[i];
-    s.candidates = ws.last.n_cand;
+    s.candidates = ws.last.cands;
 }
 
-void record_stats(issl_index* ix, Workspace& ws) {
+issl_score_stats run_stats(issl_index* ix, Workspace& ws) {
     float scan = 0.f, total = 0.f;
-    cudaEventElapsedTime(&scan, ws.ev[1], ws.ev[2]);
-    cudaEventElapsedTime(&total, ws.ev[0], ws.ev[3]);
-    fill_stats(ws, scan, total, ws.launches, ix->stats);
+    const size_t waves = slice_waves(ix).size();
+    for (size_t w = 0; w < waves; w++) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ws.ev[2 + 2 * w], ws.ev[3 + 2 * w]);
+        scan += t;
+    }
+    cudaEventElapsedTime(&total, ws.ev[0], ws.ev[1]);
+    issl_score_stats s{};
+    fill_stats(ws, scan, total, ws.launches, s);
     ws.launches = 0;
+    return s;
 }
 
+void add_stats(issl_score_stats& a, const issl_score_stats& b) {
+    a.scan_ms += b.scan_ms;
+    a.total_ms += b.total_ms;
+    a.probes += b.probes;
+    a.buckets_scanned += b.buckets_scanned;
+    a.entries_scanned += b.entries_scanned;
+    a.units += b.units;
+    a.hits += b.hits;
+    a.scan_bytes += b.scan_bytes;
+    a.launches += b.launches;
+    for (int i = 0; i < 3; i++) a.class_probes[i] += b.class_probes[i];
+    a.candidates += b.candidates;
+}
+
+// One pipeline run over n guides, growing the workspace and rerunning on overflow.
+issl_score_stats run_once(issl_index* ix, Workspace& ws, RunSpec R, uint64_t* d_distinct, cudaStream_t st) {
+    for (int attempt = 0; attempt < 4; attempt++) {
+        ensure_capacity(ix, ws, R.n, false, st);
+        ws.launches += enqueue_pipeline(ix, ws, R, st);
+        if (d_distinct && R.distinct_last) {
+            k_copy_distinct<<<1, 1, 0, st>>>(ws.counters.p, d_distinct);
+            ws.launches++;
+        }
+        if (check_and_grow(ws, st)) return run_stats(ix, ws);
+    }
+    throw Error(ISSL_ERR_NOMEM, "scoring workspace kept overflowing");
+}
+
+// Guides per pipeline run: all of them unless ISSL_MAX_GUIDES_PER_RUN caps it (a way to bound the
+// workspace of very large calls up front).
+uint64_t initial_chunk(uint64_t n) {
+    if (const char* e = std::getenv("ISSL_MAX_GUIDES_PER_RUN")) {
+        const long long v = std::atoll(e);
+        if (v > 0 && static_cast<uint64_t>(v) < n) return static_cast<uint64_t>(v);
+    }
+    return n;
+}
+
+// Scores the guides in one run, or, when the device cannot hold the workspace a run needs (the
+// candidates of many promiscuous guides), in consecutive chunks of guides, halving the chunk
+// until it fits. Results do not depend on the split.
 void run_scoring(issl_index* ix, const uint64_t* d_qsig_in, uint64_t n, const ScoreParams& P, double* d_mit,
                  double* d_cfd, char* d_code, uint64_t* d_count, uint64_t* d_distinct, cudaStream_t st) {
     Workspace& ws = workspace(ix);
     if (P.want_distinct) ws.bitmap.reserve(ix->n_sites / 32 + 1);
-    RunSpec R;
-    R.qsig = d_qsig_in;
-    R.n = n;
-    R.P = P;
-    R.mit = d_mit;
-    R.cfd = d_cfd;
-    R.code = d_code;
-    R.count = d_count;
-    for (int attempt = 0; attempt < 4; attempt++) {
-        ensure_capacity(ix, ws, n, false, st);
-        ws.launches += enqueue_pipeline(ix, ws, R, st);
-        if (d_distinct) {
-            k_copy_distinct<<<1, 1, 0, st>>>(ws.counters.p, d_distinct);
-            ws.launches++;
+    issl_score_stats sum{};
+    uint64_t chunk = initial_chunk(n), done = 0;
+    while (done < n) {
+        const uint64_t k = std::min(chunk, n - done);
+        RunSpec R;
+        R.qsig = d_qsig_in + done;
+        R.n = k;
+        R.P = P;
+        R.mit = d_mit ? d_mit + done : nullptr;
+        R.cfd = d_cfd ? d_cfd + done : nullptr;
+        R.code = d_code + done;
+        R.count = d_count ? d_count + done : nullptr;
+        R.distinct_first = done == 0;
+        R.distinct_last = done + k == n;
+        try {
+            add_stats(sum, run_once(ix, ws, R, d_distinct, st));
+        } catch (const Error& e) {
+            if (e.code != ISSL_ERR_NOMEM || k == 1) throw;
+            chunk = (k + 1) / 2;
+            continue;
         }
-        if (check_and_grow(ws, st)) {
-            record_stats(ix, ws);
-            return;
-        }
+        done += k;
     }
-    throw Error(ISSL_ERR_NOMEM, "scoring workspace kept overflowing");
+    ix->stats = sum;
 }
 
 }  // namespace
@@ -1664,6 +1857,44 @@ void run_batch(issl_batch* b, uint64_t n, const issl_guide_set* sets, size_t n_s
     throw Error(ISSL_ERR_NOMEM, "scoring workspace kept overflowing");
 }
 
+// Scores a batch in consecutive chunks of guides (one chunk unless the device cannot hold the
+// workspace the whole batch needs; then the chunk is halved until it fits). load(offset, k) puts
+// the chunk's signatures into the workspace, store(offset, k) hands its results out.
+template <class Load, class Store>
+void run_batch_chunked(issl_batch* b, uint64_t n, const issl_guide_set* sets, size_t n_sets, cudaStream_t st,
+                       Load load, Store store) {
+    Workspace& ws = *b->ws;
+    issl_score_stats sum{};
+    uint64_t chunk = initial_chunk(n), done = 0;
+    while (done < n) {
+        const uint64_t k = std::min(chunk, n - done);
+        std::vector<issl_guide_set> sub;  // the sets, cut to [done, done + k)
+        uint64_t pos = 0;
+        for (size_t i = 0; i < n_sets; i++) {
+            const uint64_t lo = std::max(pos, done), hi = std::min(pos + sets[i].count, done + k);
+            if (hi > lo) {
+                issl_guide_set t = sets[i];
+                t.count = hi - lo;
+                sub.push_back(t);
+            }
+            pos += sets[i].count;
+        }
+        try {
+            ensure_capacity(b->ix, ws, k, true, st);
+            load(done, k);
+            run_batch(b, k, sub.data(), sub.size(), st);
+            store(done, k);
+        } catch (const Error& e) {
+            if (e.code != ISSL_ERR_NOMEM || k == 1) throw;
+            chunk = (k + 1) / 2;
+            continue;
+        }
+        add_stats(sum, b->stats);
+        done += k;
+    }
+    b->stats = sum;
+}
+
 void check_sets(uint64_t n, const issl_guide_set* sets, size_t n_sets) {
     ISSL_REQUIRE(n_sets >= 1 && n_sets <= kMaxSets, ISSL_ERR_ARG, "a batch holds 1..65535 guide sets");
     ISSL_REQUIRE(sets, ISSL_ERR_ARG, "issl_batch_score: null set table");
@@ -1763,6 +1994,15 @@ int issl_workspace_bytes(const issl_index* ix, uint64_t n, double candidates_per
     });
 }
 
+int issl_index_trim(issl_index* ix) {
+    return guarded([&] {
+        ISSL_REQUIRE(ix, ISSL_ERR_ARG, "issl_index_trim: null argument");
+        ISSL_CUDA(cudaSetDevice(ix->device));
+        if (ix->ws) ISSL_CUDA(cudaStreamSynchronize(ix->ws->own_stream));
+        ix->ws.reset();
+    });
+}
+
 int issl_get_tuning(const issl_index* ix, issl_tuning* out) {
     return guarded([&] {
         ISSL_REQUIRE(ix && out, ISSL_ERR_ARG, "issl_get_tuning: null argument");
@@ -1778,6 +2018,8 @@ int issl_set_tuning(issl_index* ix, const issl_tuning* t) {
         ISSL_REQUIRE(t->stages >= 2 && t->stages <= static_cast<uint32_t>(issl::kMaxStages), ISSL_ERR_ARG,
                      "tuning: stages must be 2..4");
         ISSL_REQUIRE(t->blocks_per_sm <= 32, ISSL_ERR_ARG, "tuning: blocks_per_sm must be 0..32");
+        ISSL_REQUIRE(t->first_wave <= static_cast<uint32_t>(issl::kMaxSlices), ISSL_ERR_ARG,
+                     "tuning: first_wave must be 0..64");
         ix->tuning = *t;
         ix->tuning_version++;
     });
@@ -1814,13 +2056,16 @@ int issl_batch_score(issl_batch* b, const uint64_t* d_sigs, size_t n, const issl
         ISSL_CUDA(cudaSetDevice(b->ix->device));
         issl::Workspace& ws = *b->ws;
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ws.own_stream;
-        issl::ensure_capacity(b->ix, ws, n, true, st);
-        if (d_sigs != ws.qsig.p) ISSL_CUDA(cudaMemcpyAsync(ws.qsig.p, d_sigs, n * 8, cudaMemcpyDeviceToDevice, st));
-        issl::run_batch(b, n, sets, n_sets, st);
-        if (d_mit) ISSL_CUDA(cudaMemcpyAsync(d_mit, ws.out_mit.p, n * 8, cudaMemcpyDeviceToDevice, st));
-        if (d_cfd) ISSL_CUDA(cudaMemcpyAsync(d_cfd, ws.out_cfd.p, n * 8, cudaMemcpyDeviceToDevice, st));
-        ISSL_CUDA(cudaMemcpyAsync(d_code, ws.out_code.p, n, cudaMemcpyDeviceToDevice, st));
-        if (d_count) ISSL_CUDA(cudaMemcpyAsync(d_count, ws.out_count.p, n * 8, cudaMemcpyDeviceToDevice, st));
+        const auto D2D = cudaMemcpyDeviceToDevice;
+        issl::run_batch_chunked(
+            b, n, sets, n_sets, st,
+            [&](uint64_t o, uint64_t k) { ISSL_CUDA(cudaMemcpyAsync(ws.qsig.p, d_sigs + o, k * 8, D2D, st)); },
+            [&](uint64_t o, uint64_t k) {
+                if (d_mit) ISSL_CUDA(cudaMemcpyAsync(d_mit + o, ws.out_mit.p, k * 8, D2D, st));
+                if (d_cfd) ISSL_CUDA(cudaMemcpyAsync(d_cfd + o, ws.out_cfd.p, k * 8, D2D, st));
+                ISSL_CUDA(cudaMemcpyAsync(d_code + o, ws.out_code.p, k, D2D, st));
+                if (d_count) ISSL_CUDA(cudaMemcpyAsync(d_count + o, ws.out_count.p, k * 8, D2D, st));
+            });
         ISSL_CUDA(cudaStreamSynchronize(st));
     });
 }
@@ -1836,13 +2081,18 @@ int issl_batch_score_host(issl_batch* b, const uint64_t* sigs, size_t n, const i
         ISSL_CUDA(cudaSetDevice(b->ix->device));
         issl::Workspace& ws = *b->ws;
         cudaStream_t st = ws.own_stream;
-        issl::ensure_capacity(b->ix, ws, n, true, st);
-        ISSL_CUDA(cudaMemcpyAsync(ws.qsig.p, sigs, n * 8, cudaMemcpyHostToDevice, st));
-        issl::run_batch(b, n, sets, n_sets, st);
-        if (mit) ISSL_CUDA(cudaMemcpyAsync(mit, ws.out_mit.p, n * 8, cudaMemcpyDeviceToHost, st));
-        if (cfd) ISSL_CUDA(cudaMemcpyAsync(cfd, ws.out_cfd.p, n * 8, cudaMemcpyDeviceToHost, st));
-        ISSL_CUDA(cudaMemcpyAsync(code, ws.out_code.p, n, cudaMemcpyDeviceToHost, st));
-        if (count) ISSL_CUDA(cudaMemcpyAsync(count, ws.out_count.p, n * 8, cudaMemcpyDeviceToHost, st));
+        const auto D2H = cudaMemcpyDeviceToHost;
+        issl::run_batch_chunked(
+            b, n, sets, n_sets, st,
+            [&](uint64_t o, uint64_t k) {
+                ISSL_CUDA(cudaMemcpyAsync(ws.qsig.p, sigs + o, k * 8, cudaMemcpyHostToDevice, st));
+            },
+            [&](uint64_t o, uint64_t k) {
+                if (mit) ISSL_CUDA(cudaMemcpyAsync(mit + o, ws.out_mit.p, k * 8, D2H, st));
+                if (cfd) ISSL_CUDA(cudaMemcpyAsync(cfd + o, ws.out_cfd.p, k * 8, D2H, st));
+                ISSL_CUDA(cudaMemcpyAsync(code + o, ws.out_code.p, k, D2H, st));
+                if (count) ISSL_CUDA(cudaMemcpyAsync(count + o, ws.out_count.p, k * 8, D2H, st));
+            });
         ISSL_CUDA(cudaStreamSynchronize(st));
     });
 }
@@ -1924,7 +2174,6 @@ __device__ __forceinline__ void static_block(const StaticArgs& a, const SliceGeo
     const int hi = min(static_cast<int>(e1) - static_cast<int>(32 * b), 32);
     const uint32_t valid = (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
     uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), a.P.max_dist) & valid;
-    (void)NW;
     while (cbits) {
         const int e = __ffs(cbits) - 1;
         cbits &= cbits - 1;
@@ -1941,8 +2190,7 @@ __device__ __forceinline__ void static_block(const StaticArgs& a, const SliceGeo
         if (!own) continue;
         const uint32_t pos = static_cast<uint32_t>(32 * b) + e;
         const uint32_t slot = atomicAdd(cnt, 1u);
-        if (slot < kStaticHits)
-            hits[slot] = make_uint4(pos, s, rm, a.ix.ids[static_cast<uint64_t>(s) * a.ix.n_sites + pos]);
+        if (slot < kStaticHits) hits[slot] = make_uint4(pos, s, rm, 0u);
     }
 }
 
@@ -2025,8 +2273,10 @@ __global__ void __launch_bounds__(kStaticThreads) k_score_static(StaticArgs a) {
             Contribution c{0.0, 0.0, 0};
             if (t < L) {
                 const uint4 r = hits[s_keys[t] & (kStaticHits - 1)];
-                const uint4 sr = a.ix.srec[r.w];
-                c = contribution(T, a.P, q, (static_cast<uint64_t>(sr.y) << 32) | sr.x, sr.z);
+                uint32_t id, occ;
+                uint64_t sig;
+                load_site(a.ix, r.y, r.x, q, s_geom[r.y], id, occ, sig);
+                c = contribution(T, a.P, q, sig, occ);
             }
             double im = warp_incl_sum(c.mit, lane), ic = warp_incl_sum(c.cfd, lane);
             uint64_t in = warp_incl_sum_u64(c.occ, lane);

@@ -35,6 +35,7 @@ double time_tuning(Sample& s, const issl_tuning& t, issl_score_stats* last, int 
     for (int r = 0; r <= reps; r++) {
         const int rc = issl_score_device(s.ix, s.d_sigs, s.n, s.method, s.threshold, s.max_dist, s.mit.p, s.cfd.p,
                                          s.code.p, s.count.p, nullptr, nullptr);
+        if (rc == ISSL_ERR_NOMEM) return 1e30;  // this tuning needs more memory than there is: skip it
         if (rc != ISSL_OK) throw Error(rc, issl_last_error());
         issl_score_stats st{};
         issl_last_stats(s.ix, &st);
@@ -63,7 +64,8 @@ bool cache_lookup(const char* path, const std::string& key, issl_tuning& t) {
         std::istringstream in(line);
         std::string k;
         issl_tuning c{};
-        if (in >> k >> c.chunk[0] >> c.chunk[1] >> c.chunk[2] >> c.stages >> c.blocks_per_sm && k == key) {
+        if (in >> k >> c.chunk[0] >> c.chunk[1] >> c.chunk[2] >> c.stages >> c.blocks_per_sm >> c.first_wave &&
+            k == key) {
             t = c;
             found = true;
         }
@@ -75,7 +77,7 @@ void cache_store(const char* path, const std::string& key, const issl_tuning& t)
     std::ofstream f(path, std::ios::app);
     ISSL_REQUIRE(f.good(), ISSL_ERR_IO, std::string("autotune: cannot write the cache file ") + path);
     f << key << ' ' << t.chunk[0] << ' ' << t.chunk[1] << ' ' << t.chunk[2] << ' ' << t.stages << ' '
-      << t.blocks_per_sm << '\n';
+      << t.blocks_per_sm << ' ' << t.first_wave << '\n';
 }
 
 }  // namespace
@@ -139,6 +141,14 @@ extern "C" int issl_autotune(issl_index* ix, const uint64_t* d_sigs, size_t n, i
                 if (b != cur.blocks_per_sm) {
                     issl_tuning t = cur;
                     t.blocks_per_sm = b;
+                    consider(t);
+                }
+            // 4. slice waves
+            const issl_tuning cur2 = best;
+            for (uint32_t fw : {0u, 1u, 2u, 4u})
+                if (fw != cur2.first_wave) {
+                    issl_tuning t = cur2;
+                    t.first_wave = fw;
                     consider(t);
                 }
             rep.best_ms = best_ms;

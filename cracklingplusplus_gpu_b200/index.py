@@ -134,6 +134,10 @@ class Index:
     def save(self, path: str) -> None:
         check(lib().issl_save(self._h, path.encode()))
 
+    def trim(self) -> None:
+        """Frees the index's own scoring workspace (re-created by the next scoring call)."""
+        check(lib().issl_index_trim(self._h))
+
     def last_stats(self) -> ScoreStats:
         out = ScoreStats()
         check(lib().issl_last_stats(self._h, C.byref(out)))
@@ -145,8 +149,9 @@ class Index:
         check(lib().issl_get_tuning(self._h, C.byref(out)))
         return out
 
-    def set_tuning(self, chunk=(1024, 1024, 1024), stages: int = 3, blocks_per_sm: int = 0) -> None:
-        t = Tuning((C.c_uint32 * 3)(*chunk), stages, blocks_per_sm)
+    def set_tuning(self, chunk=(1024, 1024, 1024), stages: int = 3, blocks_per_sm: int = 0,
+                   first_wave: int = 1) -> None:
+        t = Tuning((C.c_uint32 * 3)(*chunk), stages, blocks_per_sm, first_wave)
         check(lib().issl_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, d_sigs: int, n: int, method="and", threshold: float = 75.0, max_dist: int = 4,

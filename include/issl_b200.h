@@ -53,6 +53,9 @@ typedef struct {
     uint64_t device_bytes;    /* HBM held by the resident index */
     int device;               /* CUDA ordinal holding the index */
     int min_width, max_width; /* slice widths (positions per slice) */
+    int entry_bytes;          /* 8: list entries carry the residual code (one read per scored
+                                 hit); 4: chosen when HBM is short (a second read for the
+                                 signature). ISSL_ENTRY_BYTES=4|8 in the environment forces it */
 } issl_index_info;
 
 /* Message for the last failing call on this thread ("" when none). */
@@ -105,6 +108,11 @@ int issl_score(issl_index* index, const char* seqs, size_t stride, size_t n, int
                double threshold, int max_dist, double* mit_score, double* cfd_score, char* code,
                uint64_t* count, uint64_t* distinct);
 
+/* Every scoring entry point runs the pipeline over all its guides at once, or, when the device
+ * cannot hold the workspace that needs (many guides with thousands of candidate sites), over
+ * consecutive chunks of guides, halving the chunk until it fits; results do not depend on the
+ * split. ISSL_MAX_GUIDES_PER_RUN=<n> in the environment caps the chunk from the start. */
+
 /* Same from packed signatures in host memory. */
 int issl_score_sigs(issl_index* index, const uint64_t* sigs, size_t n, int method,
                     double threshold, int max_dist, double* mit_score, double* cfd_score,
@@ -152,6 +160,11 @@ typedef struct {
     uint64_t candidates;        /* candidate slots the scan wrote, before the ownership rule */
 } issl_score_stats;
 
+/* Frees the device memory of the index's own scoring workspace (the buffers the plain
+ * issl_score* calls grow on demand); the next call re-creates it. The index stays resident.
+ * No counterpart in the reference. */
+int issl_index_trim(issl_index* index);
+
 /* Modelled device bytes of one scoring workspace (the per-call buffers of issl_score*,
  * a batch context or a server slot) holding n guides, when the scan finds `candidates_per_guide`
  * candidate sites per guide (64 is the library's first guess). No counterpart in the reference.
@@ -163,12 +176,15 @@ int issl_last_stats(const issl_index* index, issl_score_stats* out);
  * No counterpart in the reference (its CPU loop has no tiles). The scan streams each probed
  * bucket in units of up to 1024 list positions shared by up to 32 guides; `chunk` sets the unit
  * size per bucket-size class (smaller units spread a heavy bucket over more warps), `stages`
- * the depth of each warp's asynchronous copy ring, `blocks_per_sm` the persistent grid. Results
- * do not depend on the tuning; only speed does. */
+ * the depth of each warp's asynchronous copy ring, `blocks_per_sm` the persistent grid,
+ * `first_wave` the slices scored in a first wave. Results do not depend on the tuning; only
+ * speed and memory do. */
 typedef struct {
     uint32_t chunk[3];       /* buckets of < 64, 64..4095, >= 4096 entries: 256, 512 or 1024 */
     uint32_t stages;         /* 2..4 (default 3) */
     uint32_t blocks_per_sm;  /* 0 = as many as fit (default) */
+    uint32_t first_wave;     /* slices scored before the rest (default 1; 0 = all in one wave):
+                                guides whose early exit fires there never probe the later slices */
 } issl_tuning;
 int issl_get_tuning(const issl_index* index, issl_tuning* out);
 int issl_set_tuning(issl_index* index, const issl_tuning* tuning);
@@ -184,8 +200,8 @@ typedef struct {
 /* Sweeps the tuning on a sample workload (d_sigs: n guides in device memory, scored with the
  * given method / threshold / max_dist), starting from the current tuning: staging depth first,
  * then the unit size of each bucket-size class that the sample's probes reach (heaviest class
- * first), then blocks per SM, keeping a change only when the pipeline gets faster by more than
- * 2%. The winner is applied to the index and, when cache_path is not NULL, appended there under
+ * first), then blocks per SM, then the first wave, keeping a change only when the pipeline gets
+ * faster by more than 2%. The winner is applied to the index and, when cache_path is not NULL, appended there under
  * a key made of the GPU name, the index geometry and the sample size; a later call with the
  * same key reads it back without timing. */
 int issl_autotune(issl_index* index, const uint64_t* d_sigs, size_t n, int method, double threshold,

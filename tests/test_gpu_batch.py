@@ -126,16 +126,16 @@ def test_batch_with_empty_sets_and_bad_tables(native, c2):
             bt.score(q, [(50, 9, 75.0, 4)])      # no such method
 
 
-@pytest.mark.parametrize("tuning", [((256, 256, 256), 2, 0), ((512, 1024, 256), 4, 0), ((1024, 512, 512), 3, 2),
-                                    ((1024, 1024, 1024), 2, 1)])
+@pytest.mark.parametrize("tuning", [((256, 256, 256), 2, 0, 0), ((512, 1024, 256), 4, 0, 3), ((1024, 512, 512), 3, 2, 1),
+                                    ((1024, 1024, 1024), 2, 1, 36), ((1024, 1024, 1024), 3, 0, 37)])
 def test_results_do_not_depend_on_tuning(native, c2, tuning):
     z, _, ix = c2
     q = z["queries"]
     base = ix.score(q, "and", 90.0)
-    chunk, stages, bps = tuning
-    ix.set_tuning(chunk, stages, bps)
+    chunk, stages, bps, fw = tuning
+    ix.set_tuning(chunk, stages, bps, fw)
     try:
-        assert ix.get_tuning().as_tuple() == (tuple(chunk), stages, bps)
+        assert ix.get_tuning().as_tuple() == (tuple(chunk), stages, bps, fw)
         r = ix.score(q, "and", 90.0)
         with native.Batch(ix) as bt:
             rb = bt.score(q, [(len(q), "and", 90.0, 4)])
@@ -149,12 +149,42 @@ def test_results_do_not_depend_on_tuning(native, c2, tuning):
     assert r.distinct == base.distinct
 
 
+def test_guide_chunks_give_the_same_results(native, c2, monkeypatch):
+    z, _, ix = c2
+    q = z["queries"]
+    whole = ix.score(q, "and", 90.0)
+    sets = uneven_sets(q, 7)
+    with native.Batch(ix) as bt:
+        whole_b = bt.score(q, sets)
+    monkeypatch.setenv("ISSL_MAX_GUIDES_PER_RUN", "37")
+    parts = ix.score(q, "and", 90.0)
+    with native.Batch(ix) as bt:
+        parts_b = bt.score(q, sets)
+    for a, b in [(whole, parts), (whole_b, parts_b)]:
+        assert a.code == b.code and a.distinct == b.distinct
+        np.testing.assert_array_equal(a.mit, b.mit)
+        np.testing.assert_array_equal(a.cfd, b.cfd)
+        np.testing.assert_array_equal(a.count, b.count)
+
+
+def test_trim_then_score_again(native, c2):
+    z, _, ix = c2
+    q = z["queries"]
+    a = ix.score(q, "or", 75.0)
+    ix.trim()
+    b = ix.score(q, "or", 75.0)
+    assert a.code == b.code and a.distinct == b.distinct
+    np.testing.assert_array_equal(a.mit, b.mit)
+    np.testing.assert_array_equal(a.cfd, b.cfd)
+
+
 def test_invalid_tuning_rejected(native, c2):
     _, _, ix = c2
-    for bad in [((300, 1024, 1024), 3, 0), ((1024, 1024, 1024), 5, 0), ((1024, 1024, 1024), 1, 0)]:
+    for bad in [((300, 1024, 1024), 3, 0, 1), ((1024, 1024, 1024), 5, 0, 1), ((1024, 1024, 1024), 1, 0, 1),
+                ((1024, 1024, 1024), 3, 0, 65)]:
         with pytest.raises(native.IsslError):
             ix.set_tuning(*bad)
-    assert ix.get_tuning().as_tuple() == ((1024, 1024, 1024), 3, 0)
+    assert ix.get_tuning().as_tuple() == ((1024, 1024, 1024), 3, 0, 1)
 
 
 def test_autotune_and_cache(native, c2, tmp_path):

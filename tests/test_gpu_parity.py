@@ -278,3 +278,41 @@ def test_mixed_slice_widths_use_generic_scan(native, oracle):
             tm, tc, cnt, dist = oix.score(queries, METHODS[meth], t)
             ms, cs, codes = oracle.finalise(METHODS[meth], t, tm, tc)
             assert_matches(ix.score(queries, meth, t), ms, cs, codes, cnt, dist, tag=f"mixed {meth}")
+
+
+def test_large_occurrence_counts_read_from_the_site_table(native, oracle):
+    """List entries carry occurrence counts up to 6; larger ones are read from the per-site
+    table. Counts spread over 0..100000 exercise both paths against the oracle."""
+    import synth
+    from cracklingplusplus_gpu_b200.slice_configs import slice_masks
+    sites = np.unique(synth.random_sigs(synth.Stream(9, 1), 30000))
+    rng = np.random.default_rng(4)
+    occ = np.where(rng.random(len(sites)) < 0.5, rng.integers(0, 7, len(sites)),
+                   rng.integers(7, 100000, len(sites))).astype(np.uint32)
+    masks = np.array(slice_masks("slice-8-20"), np.uint64)
+    oix = oracle.Index.build(sites, occ, masks)
+    queries = np.concatenate([sites[:300], synth.random_sigs(synth.Stream(9, 2), 300)])
+    with native.Index.build(sites, occ, masks) as ix:
+        for a, b in zip(ix.export(), oix.arrays()):
+            np.testing.assert_array_equal(a, b)
+        for meth, t in [("mitAndCfd", 50.0), ("avgMitCfd", 99.0), ("cfd", 75.0)]:
+            tm, tc, cnt, dist = oix.score(queries, METHODS[meth], t)
+            ms, cs, codes = oracle.finalise(METHODS[meth], t, tm, tc)
+            res = ix.score(queries, meth, t)
+            assert_matches(res, ms, cs, codes, cnt, dist, tag=f"large occ {meth} {t}")
+        assert int(np.max(cnt)) >= 7
+
+
+def test_four_byte_entries_match(native, oracle_arrays, monkeypatch):
+    """Indexes too large for 8-byte list entries keep 4-byte ones and read signatures from the
+    site table; forced here on a small case, the results are the same."""
+    z, meta = load_case("c1_small")
+    monkeypatch.setenv("ISSL_ENTRY_BYTES", "4")
+    with native.Index.from_arrays(*oracle_arrays("c1_small")) as ix4:
+        assert ix4.info().entry_bytes == 4
+        check_golden(ix4, z, meta)
+    monkeypatch.setenv("ISSL_ENTRY_BYTES", "8")
+    with native.Index.build(z["sites"], z["occ"], z["masks"]) as ix8:
+        assert ix8.info().entry_bytes == 8
+        for a, b in zip(ix8.export(), oracle_arrays("c1_small")):
+            np.testing.assert_array_equal(a, b)

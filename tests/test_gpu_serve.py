@@ -32,8 +32,8 @@ def requests(q, seed, k):
     meths = list(METHODS)
     for _ in range(k):
         n = int(np.exp(rng.uniform(0, np.log(600))))
-        start = int(rng.integers(0, len(q) - n))
-        out.append((q[start:start + n].copy(), meths[rng.integers(5)], float(rng.choice([50.0, 75.0, 90.0])),
+        pick = rng.integers(0, len(q), n)  # guides drawn with repetition from the case's queries
+        out.append((q[pick].copy(), meths[rng.integers(5)], float(rng.choice([50.0, 75.0, 90.0])),
                     int(rng.choice([4, 4, 3]))))
     return out
 
@@ -79,7 +79,7 @@ def test_mixed_requests_equal_alone_and_oracle(native, oracle, c2):
 
 def test_server_limits(native, c2):
     z, _, ix = c2
-    q = z["queries"]
+    q = np.resize(z["queries"], 1001)  # the case's guides, repeated
     with native.Server(ix, n_slots=2, max_batch_guides=1000) as srv:
         with pytest.raises(native.IsslError):
             srv.submit(q[:1001], "and", 75.0)  # above the batch limit
