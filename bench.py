@@ -70,8 +70,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default scan tuning (no autotune sweep)")
     ap.add_argument("--form", default="plain",
-                    help="plain (default: the headline line), or batched and/or served (comma-separated): the "
-                         "slice-10-37 forms, one JSON line each")
+                    help="plain (default: the headline line), or any of batched, served (the slice-10-37 forms) "
+                         "and capacity (500M sites, slice-8-28), comma-separated, one JSON line each")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the served-load run")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="request arrivals per second (Poisson)")
     return ap.parse_args()
@@ -410,6 +410,90 @@ SERVED = {"workload": "issl-score served: 300M-site slice-10-37 index, Poisson a
           "headroom_gb": 16, "slots": 3, "max_batch_guides": 131072}
 
 
+CAPACITY = {"workload": "issl-score capacity: 500M-site slice-8-28 index, 5M guides (90% random, 10% repeat-derived), "
+                        "MIT+CFD 'and', threshold 75, max 4 mismatches",
+            "n_sites": 500_000_000, "slice_config": "slice-8-28", "n_queries": 5_000_000, "copied_frac": 0.0,
+            "repeat_query_frac": 0.1, "seed": 1237, "method": "and", "threshold": 75.0, "max_dist": 4}
+
+
+def bench_capacity(args, pkg):
+    """The largest index: 500M sites x 28 slices, 5M guides in one call (chunked by the library
+    if the workspace does not fit), with a CPU parity sample when the host can hold the export."""
+    import torch
+    n_sites = args.sites or CAPACITY["n_sites"]
+    nq = args.queries or CAPACITY["n_queries"]
+    spec = pkg.SynthSpec(seed=CAPACITY["seed"], n_sites=n_sites, slice_config=CAPACITY["slice_config"],
+                         n_queries=nq, copied_frac=CAPACITY["copied_frac"],
+                         repeat_query_frac=CAPACITY["repeat_query_frac"])
+    t0 = time.time()
+    ix, q = pkg.Index.synth(spec)
+    gen_s = time.time() - t0
+    info = ix.info()
+    log(f"capacity: {n_sites} sites, {info.n_slices} slices, {info.device_bytes / 1e9:.1f} GB resident, "
+        f"{info.entry_bytes}-byte entries, generated in {gen_s:.1f} s")
+    meth = pkg.CLI_METHODS[CAPACITY["method"]]
+    thr, md = CAPACITY["threshold"], CAPACITY["max_dist"]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.Stream(device=dev)
+    d_q = torch.from_numpy(np.ascontiguousarray(q).view(np.int64)).to(dev)
+    d_mit = torch.empty(nq, dtype=torch.float64, device=dev)
+    d_cfd = torch.empty(nq, dtype=torch.float64, device=dev)
+    d_code = torch.empty(nq, dtype=torch.uint8, device=dev)
+    d_cnt = torch.empty(nq, dtype=torch.int64, device=dev)
+    sample = min(nq, 200_000)
+    tuning = None
+    if not args.no_tune:
+        t, rep = ix.autotune(d_q.data_ptr(), sample, meth, thr, md)
+        tuning = {"chunk": list(t.chunk), "stages": t.stages, "blocks_per_sm": t.blocks_per_sm,
+                  "first_wave": t.first_wave, "default_ms": rep.default_ms, "tuned_ms": rep.best_ms,
+                  "sample_guides": sample}
+        ix.trim()
+
+    def step():
+        ix.score_device(d_q.data_ptr(), nq, meth, thr, md, d_mit.data_ptr(), d_cfd.data_ptr(), d_code.data_ptr(),
+                        d_cnt.data_ptr(), 0, stream.cuda_stream)
+
+    step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(1, min(args.steps, 3))
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        torch.cuda.nvtx.range_push("timed_device")
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+    ms = ev0.elapsed_time(ev1) / steps
+    st = ix.last_stats()
+    log(f"capacity: {ms:.1f} ms per 5M-guide call")
+    res = pkg.ScoreResult(d_mit.cpu().numpy(), d_cfd.cpu().numpy(), bytes(d_code.cpu().numpy()),
+                          d_cnt.cpu().numpy().view(np.uint64), None)
+    parity = None
+    import psutil
+    need = n_sites * info.n_slices * 8 * 1.3
+    if not args.no_cpu and psutil.virtual_memory().available > need:
+        cpu, parity = cpu_baseline_port(ix, q, meth, thr, min(args.cpu_seconds, 20.0), res)
+        parity["cpu_guides_per_s"] = cpu["value"]
+        parity["cpu_cores"] = cpu["cores"]
+    else:
+        parity = {"skipped": f"host memory {psutil.virtual_memory().available / 1e9:.0f} GB < {need / 1e9:.0f} GB "
+                             "for the exported index"}
+    ix.close()
+    return {
+        "metric": "guides/sec, capacity run (500M-site slice-8-28 index, 5M guides, 1 B200)",
+        "value": nq / (ms / 1e3), "unit": "guides/s", "n_gpus": 1, "steps": steps, "ms_per_step": ms,
+        "higher_is_better": True, "dtype": "u32/u64 integer scan, f64 sums",
+        "data": "synthetic (seeded, generated on device)",
+        "config": dict(CAPACITY, n_sites=n_sites, n_queries=nq, entry_bytes=info.entry_bytes,
+                       resident_gb=info.device_bytes / 1e9, generation_s=gen_s),
+        "stats": {"scan_ms": st.scan_ms, "scan_bytes": st.scan_bytes, "hits": st.hits, "candidates": st.candidates,
+                  "probes": st.probes, "launches": st.launches},
+        "tuning": tuning, "parity_sample": parity, "clocks": clocks.summary(),
+    }
+
+
 def run_forms(args, forms):
     import torch
     import cracklingplusplus_gpu_b200 as pkg
@@ -419,6 +503,11 @@ def run_forms(args, forms):
         return
     build.build()
     torch.cuda.set_device(local)
+    if "capacity" in forms:
+        print(json.dumps(bench_capacity(args, pkg)), flush=True)
+        forms = [f for f in forms if f != "capacity"]
+        if not forms:
+            return
     n_sites = args.sites or FORMS["n_sites"]
     pool = args.queries or FORMS["pool"]
     spec = pkg.SynthSpec(seed=FORMS["seed"], n_sites=n_sites, slice_config=FORMS["slice_config"], n_queries=pool,

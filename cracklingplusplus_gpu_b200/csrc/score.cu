@@ -1,24 +1,26 @@
 // ISSL scoring on the GPU: the hot path of lib/ISSLScoringModule.cpp:206-462 and
 // ISSLScoreOfftargets/ISSLScoreOfftargets.cpp:308-505.
 //
-// Pipeline (one stream, no host round trip; sizes produced on the device are read on the device):
-//   1 probe_count   every (guide, slice) pair -> its global bucket; count probes per bucket
-//   2 bucket scan   exclusive scan over all buckets of (scan units, probes): per-bucket probe
-//                   slot ranges, and unit descriptors -- a unit is (bucket chunk of kChunk
-//                   entries) x (up to kGroup guides probing that bucket), so guides sharing a
-//                   bucket read its entries once and heavy buckets split into many units
+// Pipeline (one stream, no host round trip; sizes produced on the device are read on the device),
+// run once per slice wave (the first slices, then the rest) for the guides still scoring:
+//   1 probe_count   every (guide, wave slice) pair -> its global bucket; count probes per bucket
+//   2 bucket scan   exclusive scan over the wave's buckets of (scan units, probes): per-bucket
+//                   probe slot ranges, and unit descriptors -- a unit is (bucket chunk of up to
+//                   kChunk entries) x (up to kGroup guides probing that bucket), so guides sharing
+//                   a bucket read its entries once and heavy buckets split into many units
 //   3 probe_scatter guides grouped by bucket, with each guide's residual code for that slice
-//   4 scan          stream the residual codes of every unit with 128-bit loads; a candidate is
-//                   an entry whose residual differs from the guide's in <= max_dist bases.
-//                   Candidates are kept only in the first slice that reaches them (ownership
-//                   rule, replacing the per-guide toggle bitset of :252-258): site reached in
-//                   slice s is counted iff no earlier slice s' has all its positions matching
-//   5 hit offsets   per-guide hit counts -> segment offsets
-//   6 hit_scatter   hits grouped per guide
-//   7 score         per guide: order its hits as the reference visits them (slice, then list
-//                   position), accumulate MIT / CFD in FP64 with warp prefix sums, stop at the
-//                   first hit where the reference's early-exit test fires (:366-395), finalise
-//                   the scores and accept code (:404-459)
+//   4 scan          persistent, work-stealing: stream the bit-sliced residual codes of every unit
+//                   through per-warp bulk-copy rings; a candidate is an entry whose residual
+//                   differs from the guide's in <= max_dist bases
+//   5 ownership     a candidate is kept only in the first slice that reaches it (replacing the
+//                   per-guide toggle bitset of :252-258): site reached in slice s is counted iff
+//                   no earlier slice has all its positions matching; counted per guide
+//   6 hit offsets   per-guide hit counts -> segment offsets
+//   7 hit_scatter   hits grouped per guide: site id, occurrences and signature from the list entry
+//   8 score         per guide: exact fixed-point totals over the wave's hits plus the earlier
+//                   waves'; guides whose early-exit test (:366-395) fires are ordered as the
+//                   reference visits them (slice, then list position) to find the exact stop;
+//                   the others are finalised (:404-459) after the last wave or carried on
 #include <cuda_runtime.h>
 
 #include <algorithm>
