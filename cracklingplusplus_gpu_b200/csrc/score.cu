@@ -185,6 +185,7 @@ struct issl::Workspace {
     Counters last{};
     uint64_t launches = 0;  // kernels enqueued by the current call
     uint32_t tuning_version = ~0u;  // version of the index's tuning the scan is configured for
+    double cand_density = 64.0;     // candidate slots per guide the largest wave needed so far
     uint64_t epoch = 0;             // bumped whenever a buffer is reallocated
     // batch form: set table (header + sets) on the device and its pinned host staging, the
     // guide -> set map, and the captured pipeline
@@ -1410,9 +1411,11 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
         ws.unit_cap = want_units;
         ws.epoch++;
     }
-    // candidates: a first guess plus one slab of slack per scan warp; grown on demand
+    // candidates: the density earlier runs needed (64 per guide at first) plus one slab of slack
+    // per scan warp; grown on demand
     const size_t want_cands = std::max<size_t>(
-        ws.cand_cap, n * 64 + 65536 + static_cast<size_t>(ws.scan_blocks) * kScanWarps * kCandSlab);
+        ws.cand_cap, static_cast<size_t>(static_cast<double>(n) * ws.cand_density * 1.1) + 65536 +
+                         static_cast<size_t>(ws.scan_blocks) * kScanWarps * kCandSlab);
     if (ws.cand_cap < want_cands) {
         ws.cands.reserve(want_cands);
         ws.seg.reserve(want_cands);
@@ -1712,14 +1715,42 @@ issl_score_stats run_once(issl_index* ix, Workspace& ws, RunSpec R, uint64_t* d_
     throw Error(ISSL_ERR_NOMEM, "scoring workspace kept overflowing");
 }
 
-// Guides per pipeline run: all of them unless ISSL_MAX_GUIDES_PER_RUN caps it (a way to bound the
-// workspace of very large calls up front).
-uint64_t initial_chunk(uint64_t n) {
+// After a run of k guides that needed more candidate slots than the device can hold: the chunk
+// of guides whose candidates fit in about 3/4 of the free memory, at the demand the failed run
+// measured (its candidate counter keeps counting past the buffer), never more than half of k.
+uint64_t shrunk_chunk(Workspace& ws, uint64_t k) {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const double per_slot = sizeof(uint4) * 2 + sizeof(uint64_t);  // candidate, grouped hit, signature
+    const double afford = 0.75 * static_cast<double>(free_b) / per_slot;
+    const double demand = static_cast<double>(std::max<uint64_t>(ws.last.max_cand, 1));
+    ws.cand_density = std::max(ws.cand_density, demand / static_cast<double>(k));  // size the next run right
+    uint64_t c = static_cast<uint64_t>(static_cast<double>(k) * std::min(0.5, afford / demand));
+    return std::max<uint64_t>(c, 1);
+}
+
+// Guides per pipeline run: all of them, unless their candidates (at the density earlier runs
+// measured) would not fit in about 3/4 of the free memory plus the buffers already held, or
+// ISSL_MAX_GUIDES_PER_RUN caps it.
+uint64_t initial_chunk(const Workspace& ws, uint64_t n) {
+    uint64_t c = n;
     if (const char* e = std::getenv("ISSL_MAX_GUIDES_PER_RUN")) {
         const long long v = std::atoll(e);
-        if (v > 0 && static_cast<uint64_t>(v) < n) return static_cast<uint64_t>(v);
+        if (v > 0 && static_cast<uint64_t>(v) < c) c = static_cast<uint64_t>(v);
     }
-    return n;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        const double per_slot = sizeof(uint4) * 2 + sizeof(uint64_t);
+        const double afford = 0.75 * static_cast<double>(free_b) / per_slot + static_cast<double>(ws.cand_cap);
+        const double fit = afford / (ws.cand_density * 1.1);
+        if (fit < static_cast<double>(c)) c = std::max<uint64_t>(static_cast<uint64_t>(fit), 1);
+    }
+    return c;
+}
+
+// Remembers the candidate density of a successful run of k guides.
+void learn_density(Workspace& ws, uint64_t k) {
+    if (k) ws.cand_density = std::max(ws.cand_density, static_cast<double>(ws.last.max_cand) / static_cast<double>(k));
 }
 
 // Scores the guides in one run, or, when the device cannot hold the workspace a run needs (the
@@ -1730,7 +1761,7 @@ void run_scoring(issl_index* ix, const uint64_t* d_qsig_in, uint64_t n, const Sc
     Workspace& ws = workspace(ix);
     if (P.want_distinct) ws.bitmap.reserve(ix->n_sites / 32 + 1);
     issl_score_stats sum{};
-    uint64_t chunk = initial_chunk(n), done = 0;
+    uint64_t chunk = initial_chunk(ws, n), done = 0;
     while (done < n) {
         const uint64_t k = std::min(chunk, n - done);
         RunSpec R;
@@ -1747,9 +1778,10 @@ void run_scoring(issl_index* ix, const uint64_t* d_qsig_in, uint64_t n, const Sc
             add_stats(sum, run_once(ix, ws, R, d_distinct, st));
         } catch (const Error& e) {
             if (e.code != ISSL_ERR_NOMEM || k == 1) throw;
-            chunk = (k + 1) / 2;
+            chunk = shrunk_chunk(ws, k);
             continue;
         }
+        learn_density(ws, k);
         done += k;
     }
     ix->stats = sum;
@@ -1867,7 +1899,7 @@ void run_batch_chunked(issl_batch* b, uint64_t n, const issl_guide_set* sets, si
                        Load load, Store store) {
     Workspace& ws = *b->ws;
     issl_score_stats sum{};
-    uint64_t chunk = initial_chunk(n), done = 0;
+    uint64_t chunk = initial_chunk(ws, n), done = 0;
     while (done < n) {
         const uint64_t k = std::min(chunk, n - done);
         std::vector<issl_guide_set> sub;  // the sets, cut to [done, done + k)
@@ -1888,10 +1920,11 @@ void run_batch_chunked(issl_batch* b, uint64_t n, const issl_guide_set* sets, si
             store(done, k);
         } catch (const Error& e) {
             if (e.code != ISSL_ERR_NOMEM || k == 1) throw;
-            chunk = (k + 1) / 2;
+            chunk = shrunk_chunk(ws, k);
             continue;
         }
         add_stats(sum, b->stats);
+        learn_density(ws, k);
         done += k;
     }
     b->stats = sum;
