@@ -27,7 +27,7 @@ from ._lib import (  # noqa: F401
     library_path,
 )
 from .batch import Batch  # noqa: F401
-from .index import Index, ScoreResult, SynthSpec, tables  # noqa: F401
+from .index import Index, ScoreResult, SynthSpec, extract_offtargets, tables  # noqa: F401
 from .module import CracklingConfig, GuideResults, ISSLScoringModule  # noqa: F401
 from .server import Server  # noqa: F401
 from .slice_configs import SLICE_CONFIGS, slice_masks  # noqa: F401

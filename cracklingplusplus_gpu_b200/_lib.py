@@ -122,6 +122,8 @@ SIGNATURES = [
     ("issl_batch_stats", C.c_int, [vp, P(ScoreStats)]),
     ("issl_workspace_bytes", C.c_int, [vp, C.c_uint64, C.c_double, u64p]),
     ("issl_index_trim", C.c_int, [vp]),
+    ("issl_extract_offtargets", C.c_int, [P(C.c_char_p), C.c_size_t, C.c_char_p, C.c_int, u64p]),
+    ("issl_build_from_sequences", C.c_int, [P(C.c_char_p), C.c_size_t, u64p, C.c_uint64, C.c_int, P(vp), u64p]),
     ("issl_server_create", C.c_int, [vp, P(ServerConfig), P(vp)]),
     ("issl_server_submit", C.c_int, [vp, u64p, C.c_size_t, C.c_int, C.c_double, C.c_int, u64p]),
     ("issl_server_wait", C.c_int, [vp, C.c_uint64, C.c_int, f64p, f64p, C.c_char_p, u64p, P(RequestInfo)]),

@@ -17,7 +17,8 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libissl_b200.so")
 CLI = os.path.join(HERE, "issl_score_offtargets")
-SOURCES = ["index.cu", "score.cu", "radix_sort.cu", "synth.cu", "tables.cpp", "module.cpp", "tune.cpp", "serve.cpp"]
+EXTRACT_CLI = os.path.join(HERE, "issl_extract_offtargets")
+SOURCES = ["index.cu", "score.cu", "radix_sort.cu", "synth.cu", "tables.cpp", "module.cpp", "tune.cpp", "serve.cpp", "extract.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -72,6 +73,11 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
            "-Xlinker", "-rpath,$ORIGIN"]
     subprocess.run(cmd, check=True)
     os.replace(CLI + ".tmp", CLI)
+    # the command-line mirror of ExtractOfftargets
+    cmd = [NVCC, *FLAGS, os.path.join(CSRC, "extract_cli.cpp"), "-o", EXTRACT_CLI + ".tmp", "-L" + HERE,
+           "-lissl_b200", "-Xlinker", "-rpath,$ORIGIN"]
+    subprocess.run(cmd, check=True)
+    os.replace(EXTRACT_CLI + ".tmp", EXTRACT_CLI)
     return LIB
 
 

@@ -82,6 +82,18 @@ class Index:
         return cls(h.value)
 
     @classmethod
+    def from_sequences(cls, inputs, slice_masks, device: int = 0):
+        """Extracts the off-target sites of FASTA / plain-text files or directories on the GPU
+        and builds the index from them; returns (index, number of sites extracted)."""
+        paths = [p.encode() for p in inputs]
+        arr = (C.c_char_p * len(paths))(*paths)
+        m = np.ascontiguousarray(slice_masks, dtype=np.uint64)
+        h = C.c_void_p()
+        n = C.c_uint64()
+        check(lib().issl_build_from_sequences(arr, len(paths), _u64(m), len(m), device, C.byref(h), C.byref(n)))
+        return cls(h.value), n.value
+
+    @classmethod
     def synth(cls, spec: SynthSpec, device: int = 0):
         """Generates the workload on the device; returns (index, query signatures)."""
         from .slice_configs import slice_masks
@@ -206,6 +218,16 @@ class Index:
                                       C.c_void_p(d_mit or None), C.c_void_p(d_cfd or None), C.c_void_p(d_code),
                                       C.c_void_p(d_count or None), C.c_void_p(d_distinct or None),
                                       C.c_void_p(stream or None)))
+
+
+def extract_offtargets(inputs, out_path: str, device: int = 0) -> int:
+    """ExtractOfftargets on the GPU: writes every site of the inputs, sorted, one per line;
+    returns the number of lines."""
+    paths = [p.encode() for p in inputs]
+    arr = (C.c_char_p * len(paths))(*paths)
+    n = C.c_uint64()
+    check(lib().issl_extract_offtargets(arr, len(paths), out_path.encode(), device, C.byref(n)))
+    return n.value
 
 
 def tables():

@@ -301,6 +301,25 @@ int issl_server_stats(issl_server* server, issl_server_summary* out, int reset);
 /* Finishes every submitted request, then stops the slots and frees their workspaces. */
 void issl_server_destroy(issl_server* server);
 
+/* ---- off-target extraction -------------------------------------------------------------------
+ * ExtractOfftargets (ExtractOfftargets/ExtractOfftargets.cpp:16-370) on the GPU. Inputs are files
+ * or directories (every file in them): a file whose first line starts with '>' is FASTA (each
+ * record's lines trimmed, upper-cased and joined), any other file holds one sequence per line.
+ * Every site matching the reference's forward pattern [ACG][ACGT]{19}[ACGT][AG]G (its first 20
+ * bases) or reverse pattern C[CT][ACGT][ACGT]{19}[TGC] (the first 20 bases of its reverse
+ * complement) is found at every position, overlaps included. */
+
+/* Writes every site, sorted, one 20-mer per line with duplicates kept: the reference's output
+ * file, byte for byte. n_offtargets (may be NULL) receives the number of lines. */
+int issl_extract_offtargets(const char* const* inputs, size_t n_inputs, const char* out_path, int device,
+                            uint64_t* n_offtargets);
+
+/* Extracts the sites and builds the resident index from them without a file in between: the
+ * distinct sites in sorted order with their counts as occurrences, as ISSLCreateIndex reads the
+ * sorted list (ISSLCreateIndex/ISSLCreateIndex.cpp:393-417), then issl_build's bucketing. */
+int issl_build_from_sequences(const char* const* inputs, size_t n_inputs, const uint64_t* slice_masks,
+                              uint64_t n_slices, int device, issl_index** out, uint64_t* n_offtargets);
+
 /* ---- synthetic workloads (benchmarks and tests) ------------------------------------------ */
 typedef struct {
     uint64_t seed;
