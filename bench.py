@@ -70,8 +70,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default scan tuning (no autotune sweep)")
     ap.add_argument("--form", default="plain",
-                    help="plain (default: the headline line), or any of batched, served (the slice-10-37 forms) "
-                         "and capacity (500M sites, slice-8-28), comma-separated, one JSON line each")
+                    help="plain (default: the headline line), or any of batched, served (the slice-10-37 forms), "
+                         "capacity (500M sites, slice-8-28) and extract (off-target extraction), comma-separated, "
+                         "one JSON line each")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the served-load run")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="request arrivals per second (Poisson)")
     return ap.parse_args()
@@ -513,6 +514,84 @@ def bench_capacity(args, pkg):
     }
 
 
+EXTRACT = {"workload": "extract: 1 Gbp synthetic genome (GC 41%, 5% copies of 2,000 repeat segments of 2 kbp, "
+                       "N runs) as 16 FASTA records of 60-nt lines -> every off-target site of both strands, "
+                       "sorted; then the same FASTA -> resident slice-8-20 index",
+           "genome_bp": 1_000_000_000, "records": 16, "seed": 1238, "slice_config": "slice-8-20"}
+
+
+def _write_genome(path, n_bp, records, seed):
+    rng = np.random.default_rng(seed)
+    lut = np.frombuffer(b"ACGT", np.uint8)
+    with open(path, "wb") as f:
+        per = n_bp // records
+        reps = lut[rng.choice(4, (2000, 2000), p=[0.295, 0.205, 0.205, 0.295])]
+        for r in range(records):
+            g = lut[rng.choice(4, per, p=[0.295, 0.205, 0.205, 0.295])]
+            for _ in range(per // 40000):  # 5% of the bases are repeat copies
+                a = int(rng.integers(0, per - 2000))
+                g[a:a + 2000] = reps[int(rng.integers(0, 2000))]
+            for _ in range(per // 1000000):
+                a = int(rng.integers(0, per - 5000))
+                g[a:a + int(rng.integers(10, 5000))] = ord("N")
+            f.write(f">chr{r}\n".encode())
+            lines = np.full((per + 59) // 60 * 61, ord("\n"), np.uint8)
+            idx = np.arange(per)
+            lines[idx + idx // 60] = g
+            f.write(lines[: per + (per + 59) // 60].tobytes())
+
+
+def bench_extract(args, pkg):
+    """ExtractOfftargets on the GPU (file to file) and FASTA to resident index, wall clock, with
+    the CPU restatement timed on a bounded prefix of the same genome."""
+    n_bp = args.sites or EXTRACT["genome_bp"]
+    work = tempfile.mkdtemp(dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        fa = os.path.join(work, "genome.fa")
+        t0 = time.time()
+        _write_genome(fa, n_bp, EXTRACT["records"], EXTRACT["seed"])
+        log(f"extract: {n_bp} bp written in {time.time() - t0:.1f} s")
+        out = os.path.join(work, "offtargets.txt")
+        pkg.extract_offtargets([fa], out)  # warm-up (context, allocations)
+        times = []
+        for _ in range(max(1, min(args.steps, 3))):
+            t0 = time.perf_counter()
+            n = pkg.extract_offtargets([fa], out)
+            times.append(time.perf_counter() - t0)
+        t_ext = min(times)
+        masks = np.array(pkg.slice_masks(EXTRACT["slice_config"]), np.uint64)
+        t0 = time.perf_counter()
+        ix, n2 = pkg.Index.from_sequences([fa], masks)
+        t_idx = time.perf_counter() - t0
+        info = ix.info()
+        ix.close()
+        # CPU restatement on a bounded prefix: the first record's first lines
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import extract_oracle
+        sample_bp = 4_000_000
+        head = os.path.join(work, "head.fa")
+        with open(fa, "rb") as f, open(head, "wb") as h:
+            h.write(f.read(sample_bp + sample_bp // 60 + 16))
+        t0 = time.perf_counter()
+        cpu_sites = len(extract_oracle.extract([head]))
+        t_cpu = time.perf_counter() - t0
+        gpu_head = os.path.join(work, "head_ot.txt")
+        pkg.extract_offtargets([head], gpu_head)
+        same = open(gpu_head, "rb").read() == extract_oracle.extract_text([head])
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    return {
+        "metric": "off-target extraction, genome bases per second (FASTA file to sorted site file, 1 B200)",
+        "value": n_bp / t_ext, "unit": "bp/s", "n_gpus": 1, "steps": len(times), "higher_is_better": True,
+        "sites": n, "sites_per_s": n / t_ext, "seconds": t_ext,
+        "fasta_to_index": {"seconds": t_idx, "sites": n2, "distinct_sites": info.n_sites,
+                           "resident_gb": info.device_bytes / 1e9},
+        "cpu_restatement": {"bp_per_s": sample_bp / t_cpu, "sample_bp": sample_bp, "sites": cpu_sites, "cores": 1,
+                            "kind": "port (Python re, the reference's regexes)", "gpu_output_equal": same},
+        "data": "synthetic (seeded)", "config": dict(EXTRACT, genome_bp=n_bp),
+    }
+
+
 def run_forms(args, forms):
     import torch
     import cracklingplusplus_gpu_b200 as pkg
@@ -524,9 +603,11 @@ def run_forms(args, forms):
     torch.cuda.set_device(local)
     if "capacity" in forms:
         print(json.dumps(bench_capacity(args, pkg)), flush=True)
-        forms = [f for f in forms if f != "capacity"]
-        if not forms:
-            return
+    if "extract" in forms:
+        print(json.dumps(bench_extract(args, pkg)), flush=True)
+    forms = [f for f in forms if f not in ("capacity", "extract")]
+    if not forms:
+        return
     n_sites = args.sites or FORMS["n_sites"]
     pool = args.queries or FORMS["pool"]
     spec = pkg.SynthSpec(seed=FORMS["seed"], n_sites=n_sites, slice_config=FORMS["slice_config"], n_queries=pool,

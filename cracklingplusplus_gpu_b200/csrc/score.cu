@@ -185,7 +185,8 @@ struct issl::Workspace {
     Counters last{};
     uint64_t launches = 0;  // kernels enqueued by the current call
     uint32_t tuning_version = ~0u;  // version of the index's tuning the scan is configured for
-    double cand_density = 64.0;     // candidate slots per guide the largest wave needed so far
+    double cand_density = 64.0;     // candidate slots per guide recent runs needed (largest wave)
+    double cand_seen = 0.0, guides_seen = 0.0;  // their decayed, size-weighted sums
     uint64_t epoch = 0;             // bumped whenever a buffer is reallocated
     // batch form: set table (header + sets) on the device and its pinned host staging, the
     // guide -> set map, and the captured pipeline
@@ -1411,12 +1412,13 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
         ws.unit_cap = want_units;
         ws.epoch++;
     }
-    // candidates: the density earlier runs needed (64 per guide at first) plus one slab of slack
-    // per scan warp; grown on demand
-    const size_t want_cands = std::max<size_t>(
-        ws.cand_cap, static_cast<size_t>(static_cast<double>(n) * ws.cand_density * 1.1) + 65536 +
-                         static_cast<size_t>(ws.scan_blocks) * kScanWarps * kCandSlab);
+    // candidates: the density recent runs needed (64 per guide at first) plus one slab of slack
+    // per scan warp; grown by at least half when it grows (every reallocation synchronises the
+    // device, which stalls concurrent work); grown on demand after an overflow
+    size_t want_cands = static_cast<size_t>(static_cast<double>(n) * ws.cand_density * 1.1) + 65536 +
+                        static_cast<size_t>(ws.scan_blocks) * kScanWarps * kCandSlab;
     if (ws.cand_cap < want_cands) {
+        want_cands = std::max<size_t>(want_cands, ws.cand_cap + ws.cand_cap / 2);
         ws.cands.reserve(want_cands);
         ws.seg.reserve(want_cands);
         ws.segsig.reserve(want_cands);
@@ -1715,6 +1717,16 @@ issl_score_stats run_once(issl_index* ix, Workspace& ws, RunSpec R, uint64_t* d_
     throw Error(ISSL_ERR_NOMEM, "scoring workspace kept overflowing");
 }
 
+// Remembers the candidate density of a run of k guides that needed `cands` slots: a size-weighted
+// average over recent runs (halved at every run), at least 64 per guide.
+void learn_density(Workspace& ws, uint64_t k, double cands) {
+    if (!k) return;
+    ws.cand_seen = 0.5 * ws.cand_seen + cands;
+    ws.guides_seen = 0.5 * ws.guides_seen + static_cast<double>(k);
+    ws.cand_density = std::max(64.0, ws.cand_seen / ws.guides_seen);
+}
+void learn_density(Workspace& ws, uint64_t k) { learn_density(ws, k, static_cast<double>(ws.last.max_cand)); }
+
 // After a run of k guides that needed more candidate slots than the device can hold: the chunk
 // of guides whose candidates fit in about 3/4 of the free memory, at the demand the failed run
 // measured (its candidate counter keeps counting past the buffer), never more than half of k.
@@ -1724,7 +1736,7 @@ uint64_t shrunk_chunk(Workspace& ws, uint64_t k) {
     const double per_slot = sizeof(uint4) * 2 + sizeof(uint64_t);  // candidate, grouped hit, signature
     const double afford = 0.75 * static_cast<double>(free_b) / per_slot;
     const double demand = static_cast<double>(std::max<uint64_t>(ws.last.max_cand, 1));
-    ws.cand_density = std::max(ws.cand_density, demand / static_cast<double>(k));  // size the next run right
+    learn_density(ws, k, demand);  // size the next run from what this one needed
     uint64_t c = static_cast<uint64_t>(static_cast<double>(k) * std::min(0.5, afford / demand));
     return std::max<uint64_t>(c, 1);
 }
@@ -1738,6 +1750,10 @@ uint64_t initial_chunk(const Workspace& ws, uint64_t n) {
         const long long v = std::atoll(e);
         if (v > 0 && static_cast<uint64_t>(v) < c) c = static_cast<uint64_t>(v);
     }
+    // the usual case: the buffers already held fit the call, no need to ask the driver (the query
+    // is slow and would stall concurrent work)
+    const double need = static_cast<double>(c) * ws.cand_density * 1.1;
+    if (need <= static_cast<double>(ws.cand_cap)) return c;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         const double per_slot = sizeof(uint4) * 2 + sizeof(uint64_t);
@@ -1748,10 +1764,6 @@ uint64_t initial_chunk(const Workspace& ws, uint64_t n) {
     return c;
 }
 
-// Remembers the candidate density of a successful run of k guides.
-void learn_density(Workspace& ws, uint64_t k) {
-    if (k) ws.cand_density = std::max(ws.cand_density, static_cast<double>(ws.last.max_cand) / static_cast<double>(k));
-}
 
 // Scores the guides in one run, or, when the device cannot hold the workspace a run needs (the
 // candidates of many promiscuous guides), in consecutive chunks of guides, halving the chunk
