@@ -49,13 +49,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
+// Same with a suspend-time hint: a waiting warp sleeps until the phase completes or about
+// `hint_ns` nanoseconds pass, instead of spending issue slots on retries.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits for the phase of `parity` to complete; gives up after ~timeout_cycles SM clocks.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long timeout_cycles) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    for (uint32_t spins = 1;; spins++) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((spins & 255u) == 0 && clock64() - t0 > timeout_cycles) return false;
+    for (;;) {
+        if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
+        if (clock64() - t0 > timeout_cycles) return false;
     }
 }
 

@@ -33,42 +33,82 @@ namespace issl {
 namespace {
 
 constexpr int kSiteLen = 20;
-constexpr int kMatchLen = 23;
 constexpr uint8_t kSep = '\n';  // between sequences: not a base, so no match spans it
 
 // ---- host: inputs -> sequences ------------------------------------------------------------
-// boost::algorithm::trim / to_upper on ASCII (std::isspace / std::toupper in the C locale)
-std::string trim_upper(const std::string& s) {
-    size_t a = 0, b = s.size();
-    while (a < b && std::isspace(static_cast<unsigned char>(s[a]))) a++;
-    while (b > a && std::isspace(static_cast<unsigned char>(s[b - 1]))) b--;
-    std::string r = s.substr(a, b - a);
-    for (char& c : r) c = static_cast<char>(std::toupper(static_cast<unsigned char>(c)));
-    return r;
+// boost::algorithm::trim / to_upper on ASCII (std::isspace / std::toupper in the C locale), as a
+// table over bytes
+struct CharTables {
+    bool space[256];
+    char upper[256];
+    CharTables() {
+        for (int c = 0; c < 256; c++) {
+            space[c] = std::isspace(c) != 0;
+            upper[c] = static_cast<char>(std::toupper(c));
+        }
+    }
+};
+const CharTables& char_tables() {
+    static const CharTables t;
+    return t;
+}
+
+// Appends line [b, e) trimmed and upper-cased, except a FASTA header line (fasta and its first
+// character is '>'); returns its first character after trimming (0 if none).
+char append_trimmed(const char* b, const char* e, bool fasta, std::string& out) {
+    const CharTables& T = char_tables();
+    while (b < e && T.space[static_cast<unsigned char>(*b)]) b++;
+    while (e > b && T.space[static_cast<unsigned char>(e[-1])]) e--;
+    if (b == e) return 0;
+    const char first = T.upper[static_cast<unsigned char>(*b)];
+    if (fasta && first == '>') return first;  // a header: not sequence
+    const size_t at = out.size();
+    out.resize(at + static_cast<size_t>(e - b));
+    char* o = &out[at];
+    for (; b < e; b++) *o++ = T.upper[static_cast<unsigned char>(*b)];
+    return first;
 }
 
 // Appends the sequences of one input file to `out`, each followed by kSep (:66-104): a file whose
 // first line starts with '>' is FASTA (records start at header lines, their lines concatenated);
-// anything else holds one sequence per line.
+// anything else holds one sequence per line. One pass over the file's bytes; lines end at '\n'
+// as std::getline ends them.
 void append_sequences(const std::string& path, std::string& out) {
-    std::ifstream in(path, std::ios::binary);
-    ISSL_REQUIRE(in.good(), ISSL_ERR_IO, "cannot open input " + path);
-    std::string line;
-    if (!std::getline(in, line)) return;
-    if (!line.empty() && line[0] == '>') {
-        while (std::getline(in, line)) {
-            const std::string t = trim_upper(line);
-            if (!t.empty() && t[0] == '>')
-                out.push_back(static_cast<char>(kSep));
-            else
-                out += t;
-        }
+    FILE* fp = std::fopen(path.c_str(), "rb");
+    ISSL_REQUIRE(fp, ISSL_ERR_IO, "cannot open input " + path);
+    std::vector<char> buf;
+    {
+        std::fseek(fp, 0, SEEK_END);
+        const long size = std::ftell(fp);
+        std::fseek(fp, 0, SEEK_SET);
+        buf.resize(size > 0 ? static_cast<size_t>(size) : 0);
+        const size_t got = buf.empty() ? 0 : std::fread(buf.data(), 1, buf.size(), fp);
+        std::fclose(fp);
+        ISSL_REQUIRE(got == buf.size(), ISSL_ERR_IO, "short read of " + path);
+    }
+    if (buf.empty()) return;
+    out.reserve(out.size() + buf.size() + 16);
+    const char* p = buf.data();
+    const char* end = p + buf.size();
+    auto next_line = [&](const char*& b, const char*& e) -> bool {
+        if (p >= end) return false;
+        b = p;
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', static_cast<size_t>(end - p)));
+        e = nl ? nl : end;
+        p = nl ? nl + 1 : end;
+        return true;
+    };
+    const char *b, *e;
+    next_line(b, e);
+    if (b < e && *b == '>') {  // FASTA: the raw first line starts with '>' (the header is skipped)
+        while (next_line(b, e))
+            if (append_trimmed(b, e, true, out) == '>') out.push_back(static_cast<char>(kSep));
         out.push_back(static_cast<char>(kSep));
     } else {
         do {
-            out += trim_upper(line);
+            append_trimmed(b, e, false, out);
             out.push_back(static_cast<char>(kSep));
-        } while (std::getline(in, line));
+        } while (next_line(b, e));
     }
 }
 
@@ -94,94 +134,147 @@ std::vector<std::string> expand_inputs(const char* const* inputs, size_t n) {
 }
 
 // ---- device: matches -> keys ----------------------------------------------------------------
-__device__ __forceinline__ int base_code(uint8_t c) {  // A C G T -> 0 1 2 3, anything else -1
-    return c == 'A' ? 0 : c == 'C' ? 1 : c == 'G' ? 2 : c == 'T' ? 3 : -1;
+// Tiles of kTile positions, one 32-position word per thread. The block first packs the tile's
+// bases (and the word after it, which the last windows reach into) into shared memory: per word,
+// the 2-bit codes (A C G T -> 0 1 2 3, base j at bits 2j) and three bit planes with one bit per
+// position: valid (the byte is A, C, G or T), lo and hi (the code's two bits). Each thread then
+// tests its 32 positions at once with shifts of the planes of its word and the next:
+//   forward at k   positions k..k+22 all bases, code(k) != T, code(k+21) in {A, G}, code(k+22) == G
+//   reverse at k   positions k..k+22 all bases, code(k) == C, code(k+1) in {C, T}, code(k+22) != A
+// (the reference's patterns; position k+1..k+20 / k+2..k+21 of each are [ACGT]). Keys, for the
+// matches only: base j of the 20-mer at bits 2 (19 - j), so numeric order is lexicographic order:
+//   forward  codes k..k+19, the first most significant (a 2-bit-group reversal of the window)
+//   reverse  the reverse complement of codes k+3..k+22: code k+22-j complemented (x ^ 3) as base
+//            j, which is the window's codes k+3..k+22 in place, complemented
+constexpr uint32_t kTileThreads = 256, kTile = kTileThreads * 32;
+constexpr uint32_t kTileWords = kTileThreads + 1;
+constexpr uint64_t kSeqPad = kTile + 64;  // zero bytes after the sequences: every tile read is in bounds
+constexpr uint64_t kMask40 = (1ull << 40) - 1;
+
+__device__ __forceinline__ uint32_t gather_byte_lsbs(uint32_t x) {  // bit 0 of byte i -> bit i
+    return ((x & 0x01010101u) * 0x10204080u) >> 28;
 }
 
-// Forward site at i: s[i] in ACG, s[i+1..i+20] bases, s[i+21] in AG, s[i+22] == G.
-// Reverse site at i: s[i] == C, s[i+1] in CT, s[i+2..i+21] bases, s[i+22] in CGT; the site is the
-// reverse complement of s[i+3..i+22]. Key: base j of the 20-mer at bits 2 (19 - j).
-__device__ __forceinline__ void match_at(const uint8_t* s, uint64_t i, uint64_t n, bool& fwd, bool& rev,
-                                         uint64_t& kf, uint64_t& kr) {
-    fwd = rev = false;
-    if (i + kMatchLen > n) return;
-    const uint8_t c0 = s[i], c1 = s[i + 1], c21 = s[i + 21], c22 = s[i + 22];
-    const bool f_ends = (c0 == 'A' || c0 == 'C' || c0 == 'G') && (c21 == 'A' || c21 == 'G') && c22 == 'G';
-    const bool r_ends = c0 == 'C' && (c1 == 'C' || c1 == 'T') && (c22 == 'C' || c22 == 'G' || c22 == 'T');
-    if (!f_ends && !r_ends) return;
-    bool ok = true;
-    uint64_t key = 0;
-    for (int j = 1; j <= 21; j++) {  // positions 1..21 must all be bases for either pattern
-        const int b = base_code(s[i + j]);
-        if (b < 0) {
-            ok = false;
-            break;
+__device__ __forceinline__ uint64_t msb_first(uint64_t x) {  // codes 0..19 at bits 2j -> at bits 2 (19 - j)
+    uint64_t z = __brevll(x);                                 // code j at bits 63-2j (low), 62-2j (high)
+    z = ((z >> 1) & 0x5555555555555555ull) | ((z & 0x5555555555555555ull) << 1);
+    return z >> 24;
+}
+
+struct TilePlanes {
+    uint64_t codes[kTileWords];
+    uint32_t valid[kTileWords], lo[kTileWords], hi[kTileWords];
+};
+
+// ASCII A C G T = 0x41 0x43 0x47 0x54: ((c >> 1) ^ (c >> 2)) & 3 maps them to 0 1 2 3, four bytes
+// at a time (the bits kept come from the byte itself).
+__device__ __forceinline__ void pack_tile(const uint8_t* __restrict__ s, uint64_t t0, TilePlanes& t) {
+    for (uint32_t u = threadIdx.x; u < kTileWords; u += kTileThreads) {
+        const uint4* src = reinterpret_cast<const uint4*>(s + t0 + 32ull * u);
+        const uint4 w0 = src[0], w1 = src[1];
+        const uint32_t w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+        uint64_t c = 0;
+        uint32_t v = 0, lo = 0, hi = 0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const uint32_t c4 = ((w[q] >> 1) ^ (w[q] >> 2)) & 0x03030303u;
+            const uint32_t ok4 = __vcmpeq4(w[q], 0x41414141u) | __vcmpeq4(w[q], 0x43434343u) |
+                                 __vcmpeq4(w[q], 0x47474747u) | __vcmpeq4(w[q], 0x54545454u);
+            v |= gather_byte_lsbs(ok4) << (4 * q);
+            lo |= gather_byte_lsbs(c4) << (4 * q);
+            hi |= gather_byte_lsbs(c4 >> 1) << (4 * q);
+            const uint32_t m = c4 | (c4 >> 6);  // codes 0, 1 at bits 0-3; codes 2, 3 at bits 16-19
+            c |= static_cast<uint64_t>((m & 0xFu) | ((m >> 12) & 0xF0u)) << (8 * q);
         }
-    }
-    if (!ok) return;
-    if (f_ends) {
-        for (int j = 0; j < kSiteLen; j++) key = (key << 2) | static_cast<uint64_t>(base_code(s[i + j]));
-        kf = key;
-        fwd = true;
-    }
-    if (r_ends) {
-        key = 0;
-        for (int j = 0; j < kSiteLen; j++)  // complement of s[i+22-j]
-            key = (key << 2) | static_cast<uint64_t>(3 - base_code(s[i + 22 - j]));
-        kr = key;
-        rev = true;
+        t.codes[u] = c;
+        t.valid[u] = v;
+        t.lo[u] = lo;
+        t.hi[u] = hi;
     }
 }
 
-__global__ void k_count_matches(const uint8_t* __restrict__ s, uint64_t n, uint64_t per, uint32_t* __restrict__ cnt,
-                                uint64_t nchunks) {
-    for (uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; c < nchunks;
-         c += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint32_t k = 0;
-        const uint64_t e = std::min<uint64_t>(n, (c + 1) * per);
-        for (uint64_t i = c * per; i < e; i++) {
-            bool f, r;
-            uint64_t kf, kr;
-            match_at(s, i, n, f, r, kf, kr);
-            k += f + r;
+// the forward and reverse match bits of the 32 positions of word u
+__device__ __forceinline__ void match_word(const TilePlanes& t, uint32_t u, uint32_t& fwd, uint32_t& rev) {
+    const uint64_t V = t.valid[u] | static_cast<uint64_t>(t.valid[u + 1]) << 32;
+    const uint64_t L = t.lo[u] | static_cast<uint64_t>(t.lo[u + 1]) << 32;
+    const uint64_t H = t.hi[u] | static_cast<uint64_t>(t.hi[u + 1]) << 32;
+    const uint64_t a2 = V & (V >> 1), a4 = a2 & (a2 >> 2), a8 = a4 & (a4 >> 4);
+    const uint64_t all23 = a8 & (a8 >> 8) & (a8 >> 15);  // positions k..k+22 all bases
+    fwd = static_cast<uint32_t>(all23 & ~(L & H) & ~(L >> 21) & ((H & ~L) >> 22));
+    rev = static_cast<uint32_t>(all23 & (L & ~H) & (L >> 1) & ((L | H) >> 22));
+}
+
+// the codes of the 32 positions from position k of word u
+__device__ __forceinline__ uint64_t window(const TilePlanes& t, uint32_t u, uint32_t k) {
+    return k ? (t.codes[u] >> (2 * k)) | (t.codes[u + 1] << (64 - 2 * k)) : t.codes[u];
+}
+
+// Count mode (keys == nullptr): matches per tile into cnt. Emit mode: the tile's keys from
+// off[tile] (the exclusive scan of the counts) in position order, forward before reverse at a
+// position.
+__global__ void __launch_bounds__(kTileThreads) k_pam_tiles(const uint8_t* __restrict__ s, uint64_t ntiles,
+                                                           uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off,
+                                                           uint64_t* __restrict__ keys) {
+    __shared__ TilePlanes t;
+    __shared__ uint32_t wsum[kTileThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        pack_tile(s, tile * kTile, t);
+        __syncthreads();
+        // positions at or past the end read the zero padding: never bases, never a match
+        uint32_t fwd, rev;
+        match_word(t, threadIdx.x, fwd, rev);
+        const uint32_t mine = __popc(fwd) + __popc(rev);
+        uint32_t incl = mine;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += x;
         }
-        cnt[c] = k;
-    }
-}
-
-// Keys in the reference's emission order inside a chunk (forward, then reverse, per position;
-// the order does not matter after the sort).
-__global__ void k_emit_keys(const uint8_t* __restrict__ s, uint64_t n, uint64_t per, const uint64_t* __restrict__ off,
-                            uint64_t nchunks, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
-    for (uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; c < nchunks;
-         c += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint64_t o = off[c];
-        const uint64_t e = std::min<uint64_t>(n, (c + 1) * per);
-        for (uint64_t i = c * per; i < e; i++) {
-            bool f, r;
-            uint64_t kf, kr;
-            match_at(s, i, n, f, r, kf, kr);
-            if (f) {
-                keys[o] = kf;
-                vals[o] = static_cast<uint32_t>(o);
-                o++;
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t before = incl - mine, total = 0;
+#pragma unroll
+        for (int w = 0; w < kTileThreads / 32; w++) {
+            if (w < warp) before += wsum[w];
+            total += wsum[w];
+        }
+        if (!keys) {
+            if (threadIdx.x == 0) cnt[tile] = total;
+        } else {
+            uint64_t o = off[tile] + before;
+            for (uint32_t m = fwd | rev; m; m &= m - 1) {
+                const uint32_t k = __ffs(m) - 1;
+                const uint64_t x = window(t, threadIdx.x, k);
+                if ((fwd >> k) & 1u) keys[o++] = msb_first(x & kMask40);
+                if ((rev >> k) & 1u) keys[o++] = ((x >> 6) & kMask40) ^ kMask40;
             }
-            if (r) {
-                keys[o] = kr;
-                vals[o] = static_cast<uint32_t>(o);
-                o++;
-            }
         }
+        __syncthreads();  // the planes and wsum are refilled next
     }
 }
 
-__global__ void k_keys_to_text(const uint64_t* __restrict__ keys, uint64_t n, char* __restrict__ out) {
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t k = keys[i];
-        char* o = out + i * (kSiteLen + 1);
-        for (int j = 0; j < kSiteLen; j++) o[j] = "ACGT"[(k >> (2 * (kSiteLen - 1 - j))) & 3u];
-        o[kSiteLen] = '\n';
+// 256 keys per block: their 21-byte lines are built in shared memory and stored with 16-byte
+// writes (a block's lines start at a multiple of 256 x 21 bytes, a multiple of 16).
+__global__ void __launch_bounds__(256) k_keys_to_text(const uint64_t* __restrict__ keys, uint64_t n,
+                                                      char* __restrict__ out) {
+    __shared__ __align__(16) char txt[256 * (kSiteLen + 1)];
+    for (uint64_t b0 = blockIdx.x * 256ull; b0 < n; b0 += gridDim.x * 256ull) {
+        const uint64_t i = b0 + threadIdx.x;
+        const uint32_t cnt = static_cast<uint32_t>(n - b0 < 256 ? n - b0 : 256);
+        if (i < n) {
+            const uint64_t k = keys[i];
+            char* o = txt + threadIdx.x * (kSiteLen + 1);
+            for (int j = 0; j < kSiteLen; j++) o[j] = "ACGT"[(k >> (2 * (kSiteLen - 1 - j))) & 3u];
+            o[kSiteLen] = '\n';
+        }
+        __syncthreads();
+        const uint32_t bytes = cnt * (kSiteLen + 1);
+        char* dst = out + b0 * (kSiteLen + 1);
+        for (uint32_t w = threadIdx.x; w < bytes / 16; w += 256)
+            reinterpret_cast<uint4*>(dst)[w] = reinterpret_cast<const uint4*>(txt)[w];
+        for (uint32_t c = bytes / 16 * 16 + threadIdx.x; c < bytes; c += 256) dst[c] = txt[c];
+        __syncthreads();
     }
 }
 
@@ -241,7 +334,6 @@ inline unsigned grid_for(uint64_t n, unsigned threads = 256) {
 // The sorted site keys of the inputs, on the device.
 struct Extracted {
     DevBuf<uint64_t> keys_a, keys_b;
-    DevBuf<uint32_t> vals_a, vals_b;
     uint64_t* keys = nullptr;  // sorted, n entries
     uint64_t n = 0;
 };
@@ -253,19 +345,18 @@ void extract_sorted(const std::vector<std::string>& files, Extracted& x, cudaStr
     ISSL_REQUIRE(n < (1ull << 40), ISSL_ERR_UNSUPPORTED, "inputs above 2^40 bytes");
     if (n == 0) return;
     DevBuf<uint8_t> d_seq;
-    d_seq.reserve(n + kMatchLen);
+    d_seq.reserve(n + kSeqPad);
     ISSL_CUDA(cudaMemcpyAsync(d_seq.p, seq.data(), n, cudaMemcpyHostToDevice, st));
-    ISSL_CUDA(cudaMemsetAsync(d_seq.p + n, 0, kMatchLen, st));
-    const uint64_t per = 64;  // positions per chunk
-    const uint64_t nchunks = (n + per - 1) / per;
-    ISSL_REQUIRE(nchunks < 0xFFFFFFFFull, ISSL_ERR_UNSUPPORTED, "inputs too large");
+    ISSL_CUDA(cudaMemsetAsync(d_seq.p + n, 0, kSeqPad, st));
+    const uint64_t nchunks = (n + kTile - 1) / kTile;  // tiles
     DevBuf<uint32_t> cnt;
     DevBuf<uint64_t> off, total, scan_tmp;
     cnt.reserve(nchunks);
     off.reserve(nchunks + 1);
     total.reserve(1);
     scan_tmp.reserve(kScanBlocks + 4);
-    k_count_matches<<<grid_for(nchunks), 256, 0, st>>>(d_seq.p, n, per, cnt.p, nchunks);
+    const unsigned tgrid = static_cast<unsigned>(std::min<uint64_t>(nchunks, 148ull * 8));
+    k_pam_tiles<<<tgrid, kTileThreads, 0, st>>>(d_seq.p, nchunks, cnt.p, nullptr, nullptr);
     device_scan<uint64_t, OpSum>(LoadU32As64{cnt.p}, StoreExcl64{off.p}, nullptr, nchunks, scan_tmp.p, total.p, st);
     uint64_t m = 0;
     ISSL_CUDA(cudaMemcpyAsync(&m, total.p, 8, cudaMemcpyDeviceToHost, st));
@@ -275,16 +366,14 @@ void extract_sorted(const std::vector<std::string>& files, Extracted& x, cudaStr
     if (m == 0) return;
     x.keys_a.reserve(m);
     x.keys_b.reserve(m);
-    x.vals_a.reserve(m);
-    x.vals_b.reserve(m);
-    k_emit_keys<<<grid_for(nchunks), 256, 0, st>>>(d_seq.p, n, per, off.p, nchunks, x.keys_a.p, x.vals_a.p);
+    k_pam_tiles<<<tgrid, kTileThreads, 0, st>>>(d_seq.p, nchunks, nullptr, off.p, x.keys_a.p);
     ISSL_CUDA(cudaGetLastError());
     const size_t tb = radix_sort_temp_bytes(m, true);
     DevBuf<uint8_t> temp;
     temp.reserve(tb);
     uint64_t* ko = nullptr;
     uint32_t* vo = nullptr;
-    radix_sort_pairs_u64(x.keys_a.p, x.vals_a.p, x.keys_b.p, x.vals_b.p, m, 2 * kSiteLen, temp.p, tb, st, &ko, &vo);
+    radix_sort_pairs_u64(x.keys_a.p, nullptr, x.keys_b.p, nullptr, m, 2 * kSiteLen, temp.p, tb, st, &ko, &vo);
     x.keys = ko;
     ISSL_CUDA(cudaStreamSynchronize(st));
 }
@@ -326,7 +415,7 @@ int issl_extract_offtargets(const char* const* inputs, size_t n_inputs, const ch
             h_txt.resize(lines * line);
             for (uint64_t i = 0; i < x.n; i += slab) {
                 const uint64_t k = std::min<uint64_t>(slab, x.n - i);
-                issl::k_keys_to_text<<<issl::grid_for(k), 256, 0, st>>>(x.keys + i, k, d_txt.p);
+                issl::k_keys_to_text<<<issl::grid_for(k), 256, 0, st>>>(x.keys + i, k, d_txt.p);  // 256 keys per block
                 ISSL_CUDA(cudaMemcpyAsync(h_txt.data(), d_txt.p, k * line, cudaMemcpyDeviceToHost, st));
                 ISSL_CUDA(cudaStreamSynchronize(st));
                 ISSL_REQUIRE(std::fwrite(h_txt.data(), 1, k * line, fp) == k * line, ISSL_ERR_IO,

@@ -1,4 +1,5 @@
-// Stable LSD radix sort of (key, value) pairs, 8-bit digits, for the device index builder.
+// Stable LSD radix sort of (key, value) pairs, 8-bit digits, for the device index builder (or of
+// keys alone when the value pointers are null).
 //
 // Per pass: (1) each block histograms the digit over its tile, written digit-major so that
 // (2) one exclusive scan yields every (digit, block) output offset, then (3) each block
@@ -60,7 +61,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(const K* keys, cons
             const uint64_t i = wbase + j * 32 + lane;
             const bool ok = i < n;
             k[j] = ok ? keys[i] : K(0);
-            v[j] = ok ? vals[i] : 0u;
+            v[j] = ok && vals ? vals[i] : 0u;
             d[j] = ok ? (static_cast<uint32_t>(k[j] >> shift) & 255u) : 256u;
         }
 #pragma unroll
@@ -88,7 +89,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(const K* keys, cons
             if (d[j] < 256u) {
                 const uint32_t pos = boff[d[j]] + wcnt[warp][d[j]] + r[j];
                 keys_out[pos] = k[j];
-                vals_out[pos] = v[j];
+                if (vals_out) vals_out[pos] = v[j];
             }
         }
         __syncthreads();
