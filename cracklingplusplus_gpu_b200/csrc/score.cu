@@ -153,6 +153,16 @@ __host__ __device__ inline WarpLayout warp_layout(uint32_t max_wpb, uint32_t sta
 
 }  // namespace issl
 
+// One owned hit grouped under its guide: (list position, slice, site id, occurrences) and the
+// site's signature. 32 bytes, written whole by one thread: hits land in their guide's segment in
+// arrival order, and a scattered write of less than a 32-byte sector costs a DRAM read of the
+// sector when it is evicted partly written.
+struct __align__(32) HitRec {
+    uint4 r;
+    uint64_t sig;
+    uint64_t spare;
+};
+
 struct issl::Workspace {
     int device = 0;
     cudaStream_t own_stream = nullptr;
@@ -171,9 +181,9 @@ struct issl::Workspace {
     DevBuf<uint64_t> probe_qr;  // per probe slot: guide | residual << 32 (+2 padding)
     DevBuf<uint32_t> bucket_cnt, bucket_qstart;
     DevBuf<UnitDesc> units;
-    DevBuf<uint4> cands, seg;  // candidate slots; owned hits grouped per guide
+    DevBuf<uint4> cands;  // candidate slots
+    DevBuf<HitRec> seg;   // owned hits grouped per guide
     DevBuf<uint32_t> qhits, qhoff, big, exitq;
-    DevBuf<uint64_t> segsig;  // signature of each grouped hit
     DevBuf<uint32_t> bitmap;
     DevBuf<Counters> counters;
     DevBuf<uint64_t> scan64;
@@ -713,7 +723,7 @@ struct StoreQoff {
 // the scorers read only contiguous data.
 __global__ void k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint32_t* __restrict__ qhits,
                               const uint32_t* __restrict__ qhoff, IndexView ix, const uint64_t* __restrict__ qsig,
-                              uint4* __restrict__ seg, uint64_t* __restrict__ segsig) {
+                              HitRec* __restrict__ seg) {
     __shared__ SliceGeom g[kMaxSlices];
     for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
     __syncthreads();
@@ -730,9 +740,7 @@ __global__ void k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint
         load_site(ix, sl, r.y, qsig[q], g[sl], id, occ, sig);
         // the decrement leaves qhits all zero for the next call
         const uint32_t slot = qhoff[q] + atomicSub(&qhits[q], 1u) - 1u;
-        // seg record: (list position, slice, site id, occurrences) + the site signature
-        seg[slot] = make_uint4(r.y, sl, id, occ);
-        segsig[slot] = sig;
+        seg[slot] = HitRec{make_uint4(r.y, sl, id, occ), sig, 0ull};
     }
 }
 
@@ -837,8 +845,7 @@ struct Acc;
 struct ScoreArgs {
     IndexView ix;
     const uint64_t* qsig;
-    uint4* seg;
-    uint64_t* segsig;
+    HitRec* seg;
     const uint32_t* qhoff;
     const Tables* tables;
     Counters* counters;
@@ -945,12 +952,12 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         const ScoreParams P = params_of(a, qi);
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         const uint64_t q = a.qsig[qi];
-        const uint4* seg = a.seg + h0;
-        const uint64_t* sig = a.segsig + h0;
+        const HitRec* seg = a.seg + h0;
         Fx tm{0, 0}, tc{0, 0};
         uint64_t tn = 0;
         for (uint32_t j = lane; j < L; j += 32) {
-            const FxContribution c = fx_contribution(P, T, q, seg[j], sig[j]);
+            const HitRec hr = seg[j];
+            const FxContribution c = fx_contribution(P, T, q, hr.r, hr.sig);
             tm = fx_add(tm, c.mit);
             tc = fx_add(tc, c.cfd);
             tn += c.occ;
@@ -975,7 +982,7 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         }
         if (P.want_distinct)
             for (uint32_t j = lane; j < L; j += 32) {
-                const uint32_t id = seg[j].z;
+                const uint32_t id = seg[j].r.z;
                 atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
         if (lane == 0) {
@@ -1024,12 +1031,11 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
         }
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         const uint64_t q = a.qsig[qi];
-        const uint4* seg = a.seg + h0;
-        const uint64_t* sig = a.segsig + h0;
+        const HitRec* seg = a.seg + h0;
         // counting sort of the hits by slice
         for (uint32_t t = lane; t <= S; t += 32) W.cnt[t] = 0;
         __syncwarp();
-        for (uint32_t i = lane; i < L; i += 32) atomicAdd(&W.cnt[seg[i].y], 1u);
+        for (uint32_t i = lane; i < L; i += 32) atomicAdd(&W.cnt[seg[i].r.y], 1u);
         __syncwarp();
         if (lane == 0) {
             uint32_t acc = 0;
@@ -1042,7 +1048,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             W.cnt[S] = acc;
         }
         __syncwarp();
-        for (uint32_t i = lane; i < L; i += 32) W.idx[atomicAdd(&W.cur[seg[i].y], 1u)] = static_cast<uint16_t>(i);
+        for (uint32_t i = lane; i < L; i += 32) W.idx[atomicAdd(&W.cur[seg[i].r.y], 1u)] = static_cast<uint16_t>(i);
         __syncwarp();
         bool stopped = false;
         for (uint32_t sl = 0; sl < S && !stopped; sl++) {
@@ -1051,8 +1057,8 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             Fx tm{0, 0}, tc{0, 0};
             uint64_t tn = 0;
             for (uint32_t j = lane; j < ns; j += 32) {
-                const uint32_t h = W.idx[b0 + j];
-                const FxContribution c = fx_contribution(P, T, q, seg[h], sig[h]);
+                const HitRec hr = seg[W.idx[b0 + j]];
+                const FxContribution c = fx_contribution(P, T, q, hr.r, hr.sig);
                 tm = fx_add(tm, c.mit);
                 tc = fx_add(tc, c.cfd);
                 tn += c.occ;
@@ -1063,7 +1069,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             if (!exit_test(P, fx_double(tm), fx_double(tc))) {
                 if (P.want_distinct)
                     for (uint32_t j = lane; j < ns; j += 32) {
-                        const uint32_t id = seg[W.idx[b0 + j]].z;
+                        const uint32_t id = seg[W.idx[b0 + j]].r.z;
                         atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
                     }
                 rm = tm;
@@ -1075,7 +1081,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             uint32_t P2 = 1;
             while (P2 < ns) P2 <<= 1;
             for (uint32_t j = lane; j < P2; j += 32)
-                W.keys[j] = j < ns ? (static_cast<uint64_t>(seg[W.idx[b0 + j]].x) << 10) | W.idx[b0 + j] : ~0ull;
+                W.keys[j] = j < ns ? (static_cast<uint64_t>(seg[W.idx[b0 + j]].r.x) << 10) | W.idx[b0 + j] : ~0ull;
             __syncwarp();
             for (uint32_t k = 2; k <= P2; k <<= 1) {
                 for (uint32_t j = k >> 1; j > 0; j >>= 1) {
@@ -1098,10 +1104,9 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
                 FxContribution c{{0, 0}, {0, 0}, 0};
                 uint32_t id = 0;
                 if (t < ns) {
-                    const uint32_t h = W.keys[t] & 1023u;
-                    const uint4 r = seg[h];
-                    id = r.z;
-                    c = fx_contribution(P, T, q, r, sig[h]);
+                    const HitRec hr = seg[W.keys[t] & 1023u];
+                    id = hr.r.z;
+                    c = fx_contribution(P, T, q, hr.r, hr.sig);
                 }
                 const Fx im = fx_add(fx_warp_incl(c.mit, lane), rm);
                 const Fx ic = fx_add(fx_warp_incl(c.cfd, lane), rc);
@@ -1149,15 +1154,14 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             run_n = pr.occ;
         }
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
-        uint4* seg = a.seg + h0;
-        uint64_t* sig = a.segsig + h0;
+        HitRec* seg = a.seg + h0;
         const uint64_t q = a.qsig[qi];
         uint32_t P2 = 1;
         while (P2 < L) P2 <<= 1;
         const bool in_smem = L <= static_cast<uint32_t>(kBlockHits);
         if (in_smem) {
             for (uint32_t i = threadIdx.x; i < P2; i += blockDim.x)
-                s_bkeys[i] = i < L ? (order_key(seg[i]) << kBlockIdxBits) | i : ~0ull;
+                s_bkeys[i] = i < L ? (order_key(seg[i].r) << kBlockIdxBits) | i : ~0ull;
             __syncthreads();
         }
         for (uint32_t k = 2; k <= P2; k <<= 1) {
@@ -1172,13 +1176,10 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
                             s_bkeys[partner] = x;
                         }
                     } else if (partner < L) {
-                        const uint4 x = seg[i], y = seg[partner];
-                        if (order_key(x) > order_key(y)) {
+                        const HitRec x = seg[i], y = seg[partner];
+                        if (order_key(x.r) > order_key(y.r)) {
                             seg[i] = y;
                             seg[partner] = x;
-                            const uint64_t sx = sig[i];
-                            sig[i] = sig[partner];
-                            sig[partner] = sx;
                         }
                     }
                 }
@@ -1192,9 +1193,9 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             uint32_t id = 0;
             if (t < L) {
                 const uint32_t h = in_smem ? static_cast<uint32_t>(s_bkeys[t] & ((1u << kBlockIdxBits) - 1)) : t;
-                const uint4 r = seg[h];
-                id = r.z;
-                c = fx_contribution(P, T, q, r, sig[h]);
+                const HitRec hr = seg[h];
+                id = hr.r.z;
+                c = fx_contribution(P, T, q, hr.r, hr.sig);
             }
             Fx im = fx_warp_incl(c.mit, lane), ic = fx_warp_incl(c.cfd, lane);
             uint64_t in = warp_incl_sum_u64(c.occ, lane);
@@ -1421,7 +1422,6 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
         want_cands = std::max<size_t>(want_cands, ws.cand_cap + ws.cand_cap / 2);
         ws.cands.reserve(want_cands);
         ws.seg.reserve(want_cands);
-        ws.segsig.reserve(want_cands);
         ws.cand_cap = want_cands;
         ws.epoch++;
     }
@@ -1436,7 +1436,7 @@ void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide,
     uint32_t min_chunk = kChunk;
     for (uint32_t c : ix->tuning.chunk) min_chunk = std::min(min_chunk, c);
     const uint64_t slab_slack = 148ull * 16 * kScanWarps * kCandSlab;  // one slab per scan warp, at most
-    *per_candidate = sizeof(uint4) * 2 + sizeof(uint64_t);
+    *per_candidate = sizeof(uint4) + sizeof(HitRec);
     *fixed = 8 * (G + 1) + sizeof(Tables) + sizeof(Counters) + (kScanBlocks + 4) * 12 + 4096 * sizeof(UnitDesc) +
              (65536 + slab_slack) * *per_candidate;
     // qsig, probe lists, hit counts and offsets, exit queues, outputs, set map, wave lists and
@@ -1578,14 +1578,12 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, v, ws.qhits.p, R.sets, qset);
         device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, d_n, n, ws.scan32.p, &C->hit_total,
                                      st);
-        k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, ws.qhits.p, ws.qhoff.p, v, R.qsig, ws.seg.p,
-                                               ws.segsig.p);
+        k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, ws.qhits.p, ws.qhoff.p, v, R.qsig, ws.seg.p);
         k += 7;
         ScoreArgs a;
         a.ix = v;
         a.qsig = R.qsig;
         a.seg = ws.seg.p;
-        a.segsig = ws.segsig.p;
         a.exitq = ws.exitq.p;
         a.qhoff = ws.qhoff.p;
         a.tables = ws.tables.p;
@@ -1646,7 +1644,6 @@ bool check_and_grow(Workspace& ws, cudaStream_t st) {
                          "more than 2^32 candidate sites in one slice wave; split the guides");
             ws.cands.reserve(cap);
             ws.seg.reserve(cap);
-            ws.segsig.reserve(cap);
             ws.cand_cap = cap;
             ok = false;
         }
