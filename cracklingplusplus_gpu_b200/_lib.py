@@ -27,14 +27,15 @@ class IsslError(RuntimeError):
 class IndexInfo(C.Structure):
     _fields_ = [("n_sites", C.c_uint64), ("seq_len", C.c_uint64), ("n_slices", C.c_uint64),
                 ("n_buckets", C.c_uint64), ("device_bytes", C.c_uint64), ("device", C.c_int),
-                ("min_width", C.c_int), ("max_width", C.c_int), ("entry_bytes", C.c_int)]
+                ("min_width", C.c_int), ("max_width", C.c_int), ("entry_bytes", C.c_int),
+                ("host_bytes", C.c_uint64), ("window_slices", C.c_int)]
 
 
 class ScoreStats(C.Structure):
     _fields_ = [("scan_ms", C.c_double), ("total_ms", C.c_double), ("probes", C.c_uint64),
                 ("buckets_scanned", C.c_uint64), ("entries_scanned", C.c_uint64), ("units", C.c_uint64),
                 ("hits", C.c_uint64), ("scan_bytes", C.c_uint64), ("launches", C.c_uint64),
-                ("class_probes", C.c_uint64 * 3), ("candidates", C.c_uint64)]
+                ("class_probes", C.c_uint64 * 3), ("candidates", C.c_uint64), ("staged_bytes", C.c_uint64)]
 
 
 class Tuning(C.Structure):
@@ -97,6 +98,8 @@ vp = C.c_void_p
 SIGNATURES = [
     ("issl_last_error", C.c_char_p, []),
     ("issl_open", C.c_int, [C.c_char_p, C.c_int, P(vp)]),
+    ("issl_open_mapped", C.c_int, [C.c_char_p, C.c_int, C.c_uint32, P(vp)]),
+    ("issl_index_set_list_placement", C.c_int, [vp, C.c_uint32]),
     ("issl_open_arrays", C.c_int, [u64p, C.c_uint64, C.c_uint64, u64p, C.c_uint64, u64p, u64p, C.c_int, P(vp)]),
     ("issl_build", C.c_int, [u64p, P(C.c_uint32), C.c_uint64, u64p, C.c_uint64, C.c_int, P(vp)]),
     ("issl_close", C.c_int, [vp]),

@@ -36,7 +36,7 @@ __host__ __device__ __forceinline__ uint64_t site_signature(uint64_t q, uint32_t
 // entries need the signature table too.
 __device__ __forceinline__ void load_site(const IndexView& v, uint32_t s, uint32_t pos, uint64_t q, const SliceGeom& g,
                                           uint32_t& id, uint32_t& occ, uint64_t& sig) {
-    const uint64_t j = static_cast<uint64_t>(s) * v.n_sites + pos;
+    const uint64_t j = static_cast<uint64_t>(s) * v.n_sites + pos - v.ids_base;
     if (v.entry_words == 2) {
         const uint2 e = reinterpret_cast<const uint2*>(v.ids)[j];
         id = entry_id(e.x, v.id_bits);

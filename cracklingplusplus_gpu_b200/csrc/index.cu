@@ -209,6 +209,53 @@ uint64_t count_buckets(const std::vector<SliceGeom>& g) {
     return t;
 }
 
+// Where a builder puts slice s: straight into the resident arrays, or, for a host-list index,
+// into one slice's worth of device memory that is copied out to the page-locked host arrays once
+// the slice is complete (the whole lists never need to fit on the device).
+struct SliceSink {
+    issl_index* ix;
+    DevBuf<uint32_t> ids1, rbits1;
+    explicit SliceSink(issl_index* x) : ix(x) {
+        const uint64_t N = ix->n_sites, ew = ix->entry_words, words = rbits_words(ix);
+        if (ix->host_lists) {
+            ix->h_ids.reserve(ix->n_slices * N * ew);
+            ix->h_rbits.reserve(words);
+            std::memset(ix->h_rbits.p + (words - 4), 0, 16);  // the padding words
+            uint64_t most = 0;
+            for (auto& g : ix->geom) most = std::max<uint64_t>(most, blocks_per_slice(N) * g.wpb);
+            ids1.reserve(N * ew);
+            rbits1.reserve(most);
+        } else {
+            ix->ids.reserve(ix->n_slices * N * ew);
+            ix->rbits.reserve(words);
+        }
+    }
+    uint32_t* ids(uint64_t s) { return ix->host_lists ? ids1.p : ix->ids.p + s * ix->n_sites * ix->entry_words; }
+    // slice s's geometry and array for k_rbits (the one-slice buffer starts at the slice's first word)
+    SliceGeom geom(uint64_t s) const {
+        SliceGeom g = ix->geom[s];
+        if (ix->host_lists) g.wbase = 0;
+        return g;
+    }
+    uint32_t* rbits() { return ix->host_lists ? rbits1.p : ix->rbits.p; }
+    void done(uint64_t s, cudaStream_t st) {
+        if (!ix->host_lists) return;
+        const uint64_t N = ix->n_sites, ew = ix->entry_words;
+        const SliceGeom& g = ix->geom[s];
+        ISSL_CUDA(cudaMemcpyAsync(ix->h_ids.p + s * N * ew, ids1.p, N * ew * 4, cudaMemcpyDeviceToHost, st));
+        ISSL_CUDA(cudaMemcpyAsync(ix->h_rbits.p + g.wbase, rbits1.p, blocks_per_slice(N) * g.wpb * 4,
+                                  cudaMemcpyDeviceToHost, st));
+        ISSL_CUDA(cudaStreamSynchronize(st));  // the one-slice buffers are refilled next
+    }
+};
+
+// list entry width: 8 bytes when HBM leaves room (host-list indexes always, their lists are not
+// on the device), unless ISSL_ENTRY_BYTES forces one
+uint32_t entry_words_for(const issl_index* ix) {
+    if (ix->host_lists && !std::getenv("ISSL_ENTRY_BYTES")) return 2u;
+    return choose_entry_words(ix->n_sites, ix->n_slices, rbits_words(ix) * 4);
+}
+
 // ---- sequential sources for the loader: the .issl byte stream, from a file or from arrays ----
 struct Source {
     virtual ~Source() = default;
@@ -313,10 +360,8 @@ void load_stream(issl_index* ix, Source& src, int device) {
     ISSL_CUDA(cudaMemcpyAsync(ix->d_geom.p, ix->geom.data(), S * sizeof(SliceGeom), cudaMemcpyHostToDevice, st));
 
     ix->occ.reserve(N);
-    ix->entry_words = choose_entry_words(N, S, (bitsliced_words(ix->geom, N) + 4) * 4);
-    const uint64_t ew = ix->entry_words;
-    ix->ids.reserve(S * N * ew);
-    ix->rbits.reserve(bitsliced_words(ix->geom, N) + 4);
+    ix->entry_words = entry_words_for(ix);
+    SliceSink sink(ix);
     ix->offsets.reserve(ix->n_buckets + 1);
     DevBuf<uint32_t> seen, bucket_of, flags;
     seen.reserve(N / 32 + 1);
@@ -354,14 +399,15 @@ void load_stream(issl_index* ix, Source& src, int device) {
             src.read(stg.h[b], cnt * 8, "reading slice contents failed");
             ISSL_CUDA(cudaMemcpyAsync(stg.d[b], stg.h[b], cnt * 8, cudaMemcpyHostToDevice, st));
             k_split_entries<<<grid_for(cnt), 256, 0, st>>>(stg.d[b], j, cnt, N, s == 0, g, ix->sigs.p, bucket_of.p,
-                                                           ix->ids.p + s * N * ew, ix->entry_words, ix->id_bits,
+                                                           sink.ids(s), ix->entry_words, ix->id_bits,
                                                            ix->occ_esc, ix->occ.p, seen.p, flags.p);
             ISSL_CUDA(cudaEventRecord(stg.done[b], st));
             j += cnt;
         }
-        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(ix->ids.p + s * N * ew, ix->entry_words, ix->id_bits,
-                                                                    ix->sigs.p, N, g, ix->rbits.p);
+        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(sink.ids(s), ix->entry_words, ix->id_bits,
+                                                                    ix->sigs.p, N, sink.geom(s), sink.rbits());
         ISSL_CUDA(cudaGetLastError());
+        sink.done(s, st);
         uint32_t f = 0;
         ISSL_CUDA(cudaMemcpyAsync(&f, flags.p, 4, cudaMemcpyDeviceToHost, st));
         ISSL_CUDA(cudaStreamSynchronize(st));
@@ -394,10 +440,8 @@ void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint3
     }
     ix->d_geom.reserve(S);
     ISSL_CUDA(cudaMemcpyAsync(ix->d_geom.p, ix->geom.data(), S * sizeof(SliceGeom), cudaMemcpyHostToDevice, st));
-    ix->entry_words = choose_entry_words(N, S, (bitsliced_words(ix->geom, N) + 4) * 4);
-    const uint64_t ew = ix->entry_words;
-    ix->ids.reserve(S * N * ew);
-    ix->rbits.reserve(bitsliced_words(ix->geom, N) + 4);
+    ix->entry_words = entry_words_for(ix);
+    SliceSink sink(ix);
     ix->offsets.reserve(ix->n_buckets + 1);
     DevBuf<uint32_t> keys, vals, keys2, vals2;
     DevBuf<uint8_t> temp;
@@ -416,11 +460,12 @@ void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint3
         // stable by key: ids stay ascending inside each bucket (ISSLCreateIndex.cpp:455-468)
         radix_sort_pairs_u32(keys.p, vals.p, keys2.p, vals2.p, N, 2 * g.width, temp.p, tb, st, &ko, &vo);
         k_pack_entries<<<grid_for(N), 256, 0, st>>>(vo, ix->occ.p, N, ix->id_bits, ix->occ_esc, ix->entry_words,
-                                                    ix->ids.p + s * N * ew);
+                                                    sink.ids(s));
         k_offsets_from_sorted<<<grid_for(N + 1), 256, 0, st>>>(ko, N, nb, s * N, ix->offsets.p + bbase);
-        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(ix->ids.p + s * N * ew, ix->entry_words, ix->id_bits,
-                                                                    ix->sigs.p, N, g, ix->rbits.p);
+        k_rbits<<<grid_for(blocks_per_slice(N) * 32), 256, 0, st>>>(sink.ids(s), ix->entry_words, ix->id_bits,
+                                                                    ix->sigs.p, N, sink.geom(s), sink.rbits());
         ISSL_CUDA(cudaGetLastError());
+        sink.done(s, st);
         bbase += nb;
     }
     ISSL_CUDA(cudaStreamSynchronize(st));
@@ -431,8 +476,15 @@ void export_slice_lists(const issl_index* ix, uint64_t s, uint64_t* host_lists, 
     if (!N) return;
     DevBuf<uint64_t> tmp;
     tmp.reserve(N);
-    k_join_entries<<<grid_for(N), 256, 0, st>>>(ix->ids.p + s * N * ix->entry_words, ix->entry_words, ix->id_bits,
-                                                ix->occ.p, N, tmp.p);
+    const uint32_t* ids = ix->ids.p + s * N * ix->entry_words;
+    DevBuf<uint32_t> staged;  // host-list index: the slice's entries brought to the device
+    if (ix->host_lists) {
+        staged.reserve(N * ix->entry_words);
+        ISSL_CUDA(cudaMemcpyAsync(staged.p, ix->h_ids.p + s * N * ix->entry_words, N * ix->entry_words * 4,
+                                  cudaMemcpyHostToDevice, st));
+        ids = staged.p;
+    }
+    k_join_entries<<<grid_for(N), 256, 0, st>>>(ids, ix->entry_words, ix->id_bits, ix->occ.p, N, tmp.p);
     ISSL_CUDA(cudaGetLastError());
     ISSL_CUDA(cudaMemcpyAsync(host_lists, tmp.p, N * 8, cudaMemcpyDeviceToHost, st));
     ISSL_CUDA(cudaStreamSynchronize(st));
@@ -455,6 +507,8 @@ issl::IndexView issl_index::view() const {
     v.occ = occ.p;
     v.ids = ids.p;
     v.rbits = rbits.p;
+    v.ids_base = 0;
+    v.rbits_base = 0;
     v.offsets = offsets.p;
     v.geom = d_geom.p;
     v.n_sites = n_sites;
@@ -477,6 +531,21 @@ int issl_open(const char* path, int device, issl_index** out) {
         ISSL_REQUIRE(path && out, ISSL_ERR_ARG, "issl_open: null argument");
         *out = nullptr;
         auto ix = std::make_unique<issl_index>();
+        issl::FileSource src(path);
+        issl::load_stream(ix.get(), src, device);
+        *out = ix.release();
+    });
+}
+
+int issl_open_mapped(const char* path, int device, uint32_t window_slices, issl_index** out) {
+    return guarded([&] {
+        ISSL_REQUIRE(path && out, ISSL_ERR_ARG, "issl_open_mapped: null argument");
+        ISSL_REQUIRE(window_slices >= 1 && window_slices <= static_cast<uint32_t>(issl::kMaxSlices), ISSL_ERR_ARG,
+                     "issl_open_mapped: window_slices must be 1..64");
+        *out = nullptr;
+        auto ix = std::make_unique<issl_index>();
+        ix->host_lists = true;
+        ix->window_slices = window_slices;
         issl::FileSource src(path);
         issl::load_stream(ix.get(), src, device);
         *out = ix.release();
@@ -565,6 +634,8 @@ int issl_index_get_info(const issl_index* ix, issl_index_info* out) {
         out->device_bytes = ix->sigs.bytes() + ix->occ.bytes() + ix->ids.bytes() + ix->rbits.bytes() +
                             ix->offsets.bytes() + ix->d_geom.bytes();
         out->entry_bytes = static_cast<int>(4 * ix->entry_words);
+        out->host_bytes = ix->h_ids.bytes() + ix->h_rbits.bytes();
+        out->window_slices = ix->host_lists ? static_cast<int>(ix->window_slices) : 0;
         out->device = ix->device;
         int mn = 64, mx = 0;
         for (auto& g : ix->geom) {

@@ -80,6 +80,29 @@ struct DevBuf {
     size_t bytes() const { return n * sizeof(T); }
 };
 
+// page-locked host memory (device copies from it run at full link speed)
+template <class T>
+struct PinnedBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf() { release(); }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+    }
+    void reserve(size_t count) {
+        if (count <= n && p) return;
+        release();
+        ISSL_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T)));
+        n = count;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
 // ---- slice geometry ----------------------------------------------------------------------
 // Per-slice constants. A slice is a set of `width` protospacer positions; the key of a
 // signature is the 2-bit bases at those positions packed in ascending position order
@@ -122,6 +145,9 @@ struct IndexView {  // POD view handed to kernels
     const uint32_t* ids;      // S*N list entries in list order (slice-major), entry_words words each:
                               // the packed id, then (entry_words 2) the residual code
     const uint32_t* rbits;    // bit-sliced residual codes (see SliceGeom)
+    uint64_t ids_base;        // global entry number of ids[0]: 0, or the first entry of the slice
+                              // window a host-list index has staged on the device
+    uint64_t rbits_base;      // global word number of rbits[0] (a multiple of 4), likewise
     const uint64_t* offsets;  // G+1 bucket starts in global entry numbering: s*N + position
     const SliceGeom* geom;    // S slice descriptors
     uint64_t n_sites;
@@ -145,6 +171,12 @@ struct issl_index {
     uint32_t id_bits = 32, occ_esc = 0;  // packing of the list entries (IndexView)
     uint32_t entry_words = 2;            // 32-bit words per list entry (IndexView)
     issl::DevBuf<issl::SliceGeom> d_geom;
+    // Host-list index (issl_open_mapped): ids and rbits live in page-locked host memory and are
+    // staged on the device window_slices slices at a time while scoring; the device arrays
+    // above are then empty.
+    bool host_lists = false;
+    uint32_t window_slices = 0;
+    issl::PinnedBuf<uint32_t> h_ids, h_rbits;
     std::unique_ptr<issl::Workspace> ws;
     issl_score_stats stats{};
     // scan unit size per bucket-size class, staging depth, blocks per SM, first slice wave
@@ -185,6 +217,10 @@ uint32_t choose_entry_words(uint64_t n_sites, uint64_t n_slices, uint64_t rbits_
 // builders (index.cu)
 void build_from_device_sites(issl_index* ix, const uint64_t* d_sigs, const uint32_t* d_occ,
                              cudaStream_t st);
+
+// words of the bit-sliced array: every slice's blocks, plus 4 words of padding that the scan's
+// 16-byte-rounded copies may touch
+inline uint64_t rbits_words(const issl_index* ix) { return bitsliced_words(ix->geom, ix->n_sites) + 4; }
 
 // radix sort (radix_sort.cu): stable LSD sort of (key, value) pairs on the low `bits` bits.
 size_t radix_sort_temp_bytes(size_t n, bool wide_keys);

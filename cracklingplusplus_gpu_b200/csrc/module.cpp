@@ -23,15 +23,19 @@ struct ModuleError : std::runtime_error {
 };
 
 std::mutex g_cache_mu;
-std::map<std::string, issl_index*> g_cache;  // resident indexes, keyed by (path, device)
+std::map<std::string, issl_index*> g_cache;  // indexes kept open, keyed by (path, device, mapped)
 
-issl_index* resident_index(const std::string& path, int device) {
+// The index of a path, opened on first use and kept for the process. memoryMapped selects the
+// host-list index (ISSLScoringModuleMMF's role); ISSL_WINDOW_SLICES sets its window (default 4).
+issl_index* resident_index(const std::string& path, int device, bool mapped) {
     std::lock_guard<std::mutex> lock(g_cache_mu);
-    const std::string key = path + "#" + std::to_string(device);
+    const std::string key = path + "#" + std::to_string(device) + (mapped ? "#mapped" : "");
     auto it = g_cache.find(key);
     if (it != g_cache.end()) return it->second;
     issl_index* ix = nullptr;
-    const int rc = issl_open(path.c_str(), device, &ix);
+    const char* w = std::getenv("ISSL_WINDOW_SLICES");
+    const int rc = mapped ? issl_open_mapped(path.c_str(), device, w ? static_cast<uint32_t>(std::atoi(w)) : 4u, &ix)
+                          : issl_open(path.c_str(), device, &ix);
     if (rc != ISSL_OK) throw ModuleError(rc, issl_last_error());
     g_cache[key] = ix;
     return ix;
@@ -76,7 +80,7 @@ void ISSLScoringModule::run(std::vector<guideResults>& candidateGuides) {
         std::cout << "Off-target scoring has been configured not to run. Skipping Off-target scoring" << std::endl;
         return;
     }
-    issl_index* ix = resident_index(ISSLIndex.string(), device);
+    issl_index* ix = resident_index(ISSLIndex.string(), device, config.memoryMapped);
     std::vector<size_t> picked;
     picked.reserve(candidateGuides.size());
     for (size_t i = 0; i < candidateGuides.size(); i++)
@@ -106,7 +110,7 @@ void ISSLScoringModule::run(std::vector<guideResults>& candidateGuides) {
 }
 
 extern "C" int issl_module_run(const char* index_path, int method, double threshold, int optimisation,
-                               int consensus_n, int enabled, size_t n, const char* seqs, size_t stride,
+                               int consensus_n, int flags, size_t n, const char* seqs, size_t stride,
                                const uint8_t* is_unique, const int8_t* consensus_count, const char* passed_bowtie2,
                                double* mit_out, double* cfd_out, char* code_out) {
     try {
@@ -115,7 +119,8 @@ extern "C" int issl_module_run(const char* index_path, int method, double thresh
         cfg.input.offtargetSites = index_path;
         cfg.offTarget.method = static_cast<otScoreMethod>(method);
         cfg.offTarget.scoreThreshold = threshold;
-        cfg.offTarget.enabled = enabled != 0;
+        cfg.offTarget.enabled = (flags & ISSL_MODULE_ENABLED) != 0;
+        cfg.offTarget.memoryMapped = (flags & ISSL_MODULE_MEMORY_MAPPED) != 0;
         cfg.general.optimisation = static_cast<optimisationLevel>(optimisation);
         cfg.consensus.n = static_cast<uint8_t>(consensus_n);
         std::vector<guideResults> guides(n);

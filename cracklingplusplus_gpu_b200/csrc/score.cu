@@ -166,7 +166,7 @@ struct __align__(32) HitRec {
 struct issl::Workspace {
     int device = 0;
     cudaStream_t own_stream = nullptr;
-    cudaEvent_t ev[2 + 2 * 2] = {};  // call start / end, then scan start / end of each slice wave
+    cudaEvent_t ev[2 + 2 * kMaxSlices] = {};  // call start / end, then scan start / end of each slice wave
     size_t q_cap = 0, unit_cap = 0, cand_cap = 0;
     uint64_t g_cap = 0;
     int scan_blocks = 0;
@@ -194,6 +194,7 @@ struct issl::Workspace {
     DevBuf<uint64_t> out_count, out_distinct;
     Counters last{};
     uint64_t launches = 0;  // kernels enqueued by the current call
+    uint64_t staged = 0;    // host-list index: bytes the last pipeline copies from host memory
     uint32_t tuning_version = ~0u;  // version of the index's tuning the scan is configured for
     double cand_density = 64.0;     // candidate slots per guide recent runs needed (largest wave)
     double cand_seen = 0.0, guides_seen = 0.0;  // their decayed, size-weighted sums
@@ -211,8 +212,17 @@ struct issl::Workspace {
     uint64_t graph_epoch = ~0ull;
     uint32_t graph_tuning = ~0u;
     uint64_t graph_kernels = 0;
+    // host-list index: two device windows of staged slices, the stream that fills them, and the
+    // events that order the fills with the scans (window b is free again once the hit scatter of
+    // the wave that used it has run)
+    DevBuf<uint32_t> win_ids[2], win_rbits[2];
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t win_start = nullptr, win_ready[2] = {}, win_free[2] = {};
     ~Workspace() {
         if (graph) cudaGraphExecDestroy(graph);
+        for (cudaEvent_t e : {win_start, win_ready[0], win_ready[1], win_free[0], win_free[1]})
+            if (e) cudaEventDestroy(e);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         if (h_batch) cudaFreeHost(h_batch);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
@@ -419,6 +429,7 @@ __global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig,
 // ownership rule to the masks with every lane busy and no memory gathers.
 struct ScanArgs {
     const uint32_t* rbits;
+    uint64_t rbits_base;  // global word number of rbits[0]
     const SliceGeom* geom;
     const UnitDesc* units;
     const uint64_t* probe_qr;
@@ -598,7 +609,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
             const uint32_t rbytes = nwords * 4u, qbytes = (qa1 - qa0) * 8u;
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&bar[st], rbytes + qbytes);
-            bulk_copy_g2s(rb + st * L.stage_words, a.rbits + wa, rbytes, &bar[st]);
+            bulk_copy_g2s(rb + st * L.stage_words, a.rbits + (wa - a.rbits_base), rbytes, &bar[st]);
             bulk_copy_g2s(qr + st * kStageQr, a.probe_qr + qa0, qbytes, &bar[st]);
         }
         slot++;
@@ -1356,6 +1367,47 @@ void with_alloc_guard(Workspace& ws, F&& f) {
     }
 }
 
+// Slice waves of a call: the first `first_wave` slices, then the rest (one wave when first_wave
+// is 0 or covers every slice). The reference visits slices in order and stops a guide at the hit
+// where its test fires; a guide whose test fires within the first wave never probes the later
+// slices, which bounds the work and memory of guides with thousands of hits. A host-list index
+// further cuts each wave into groups of at most window_slices slices, one device window each.
+std::vector<std::pair<uint32_t, uint32_t>> slice_waves(const issl_index* ix) {
+    const uint32_t S = static_cast<uint32_t>(ix->n_slices), fw = ix->tuning.first_wave;
+    std::vector<std::pair<uint32_t, uint32_t>> w;
+    if (fw > 0 && fw < S)
+        w = {{0u, fw}, {fw, S}};
+    else
+        w = {{0u, S}};
+    if (!ix->host_lists) return w;
+    const uint32_t W = std::max<uint32_t>(ix->window_slices, 1);
+    std::vector<std::pair<uint32_t, uint32_t>> out;
+    for (const auto& p : w)
+        for (uint32_t s = p.first; s < p.second; s += W) out.push_back({s, std::min(p.second, s + W)});
+    return out;
+}
+
+// The part of the bit-sliced array a window of slices [s0, s1) takes: from word wb0 (the slice's
+// first word rounded down to 16 bytes, as the scan's copies are) for `words` words.
+void window_rbits(const issl_index* ix, uint32_t s0, uint32_t s1, uint64_t* wb0, uint64_t* words) {
+    const uint64_t end = s1 < ix->n_slices ? ix->geom[s1].wbase : bitsliced_words(ix->geom, ix->n_sites);
+    *wb0 = ix->geom[s0].wbase & ~3ull;
+    *words = end - *wb0;
+}
+
+// Device words a window needs, over the waves of a call: entries, and bit-sliced codes plus 8
+// words for the scan's 16-byte-rounded copies at the window's end.
+void window_capacity(const issl_index* ix, uint64_t* id_words, uint64_t* code_words) {
+    *id_words = *code_words = 0;
+    if (!ix->host_lists) return;
+    for (const auto& p : slice_waves(ix)) {
+        uint64_t wb0, words;
+        window_rbits(ix, p.first, p.second, &wb0, &words);
+        *id_words = std::max<uint64_t>(*id_words, (p.second - p.first) * ix->n_sites * ix->entry_words);
+        *code_words = std::max<uint64_t>(*code_words, words + 8);
+    }
+}
+
 void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st);
 
 void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st) {
@@ -1365,6 +1417,25 @@ void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaSt
 void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st) {
     const uint64_t S = ix->n_slices, G = ix->n_buckets;
     apply_tuning(ix, ws);
+    if (ix->host_lists) {
+        if (!ws.copy_stream) {
+            ISSL_CUDA(cudaStreamCreateWithFlags(&ws.copy_stream, cudaStreamNonBlocking));
+            for (cudaEvent_t* e : {&ws.win_start, &ws.win_ready[0], &ws.win_ready[1], &ws.win_free[0], &ws.win_free[1]})
+                ISSL_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        }
+        uint64_t idw, cw;
+        window_capacity(ix, &idw, &cw);
+        for (int b = 0; b < 2; b++) {
+            if (ws.win_ids[b].n < idw || ws.win_rbits[b].n < cw) ws.epoch++;
+            ws.win_ids[b].reserve(idw);
+            ws.win_rbits[b].reserve(cw);
+        }
+    } else {
+        for (int b = 0; b < 2; b++) {
+            ws.win_ids[b].release();
+            ws.win_rbits[b].release();
+        }
+    }
     if (ws.g_cap < G + 1) {
         ws.bucket_cnt.reserve(G + 1);
         ws.bucket_qstart.reserve(G + 1);
@@ -1443,6 +1514,9 @@ void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide,
     // running totals; scan units
     *per_guide = 8 + 12 * S + 4 * 4 + (8 + 8 + 1 + 8) + 2 + 2 * 4 + 5 * 8 +
                  sizeof(UnitDesc) * 3 * S * (kChunk / min_chunk);
+    uint64_t idw, cw;  // the two slice windows of a host-list index
+    window_capacity(ix, &idw, &cw);
+    *fixed += 2 * 4 * (idw + cw);
 }
 
 namespace {
@@ -1504,19 +1578,10 @@ __global__ void k_expand_sets(const BatchHeader* __restrict__ hdr, const SetDesc
     }
 }
 
-// Slice waves of a call: the first `first_wave` slices, then the rest (one wave when first_wave
-// is 0 or covers every slice). The reference visits slices in order and stops a guide at the hit
-// where its test fires; a guide whose test fires within the first wave never probes the later
-// slices, which bounds the work and memory of guides with thousands of hits.
-std::vector<std::pair<uint32_t, uint32_t>> slice_waves(const issl_index* ix) {
-    const uint32_t S = static_cast<uint32_t>(ix->n_slices), fw = ix->tuning.first_wave;
-    if (fw > 0 && fw < S) return {{0u, fw}, {fw, S}};
-    return {{0u, S}};
-}
-
 // Enqueues the whole pipeline. Returns the number of kernels it launched.
 uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaStream_t st) {
-    const IndexView v = ix->view();
+    const IndexView v0 = ix->view();
+    const bool staged = ix->host_lists;
     const uint64_t S = ix->n_slices, G = ix->n_buckets, n = R.n;
     const bool batch = R.hdr != nullptr;
     const uint32_t* d_n = batch ? &R.hdr->n : nullptr;
@@ -1536,9 +1601,35 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
     if (R.P.want_distinct && R.distinct_first)
         ISSL_CUDA(cudaMemsetAsync(ws.bitmap.p, 0, (ix->n_sites / 32 + 1) * 4, st));
     const auto waves = slice_waves(ix);
+    ws.staged = 0;
+    // host-list index: the copy stream starts after everything already queued on st (the last
+    // call's waves may still read the windows)
+    if (staged) {
+        ISSL_CUDA(cudaEventRecord(ws.win_start, st));
+    }
     for (size_t w = 0; w < waves.size(); w++) {
         const bool first = w == 0, last = w + 1 == waves.size();
         const uint32_t s0 = waves[w].first, s1 = waves[w].second, cur = w & 1u, nxt = cur ^ 1u;
+        IndexView v = v0;
+        const int wb = static_cast<int>(w & 1u);  // device window of this wave (host-list index)
+        if (staged) {
+            // stage the wave's slices: entries and bit-sliced codes, on the copy stream, once the
+            // window is free (its previous wave's hit scatter has run)
+            const uint64_t N = ix->n_sites, ew = ix->entry_words;
+            uint64_t wbase0, words;
+            window_rbits(ix, s0, s1, &wbase0, &words);
+            cudaStream_t cs = ws.copy_stream;
+            ISSL_CUDA(cudaStreamWaitEvent(cs, w < 2 ? ws.win_start : ws.win_free[wb], 0));
+            ISSL_CUDA(cudaMemcpyAsync(ws.win_ids[wb].p, ix->h_ids.p + s0 * N * ew, (s1 - s0) * N * ew * 4,
+                                      cudaMemcpyHostToDevice, cs));
+            ISSL_CUDA(cudaMemcpyAsync(ws.win_rbits[wb].p, ix->h_rbits.p + wbase0, words * 4, cudaMemcpyHostToDevice, cs));
+            ISSL_CUDA(cudaEventRecord(ws.win_ready[wb], cs));
+            ws.staged += ((s1 - s0) * N * ew + words) * 4;
+            v.ids = ws.win_ids[wb].p;
+            v.ids_base = static_cast<uint64_t>(s0) * N;
+            v.rbits = ws.win_rbits[wb].p;
+            v.rbits_base = wbase0;
+        }
         if (!first) ISSL_CUDA(cudaMemsetAsync(C, 0, kWaveCounterBytes, st));
         if (!last) ISSL_CUDA(cudaMemsetAsync(&C->act_n[nxt], 0, 4, st));
         const WaveProbes wp{first ? nullptr : ws.active[cur].p, first ? nullptr : &C->act_n[cur], d_n, n, s0, s1 - s0};
@@ -1555,7 +1646,8 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
                                                ws.probe_qr.p);
         k += 7;
         ScanArgs sa;
-        sa.rbits = ix->rbits.p;
+        sa.rbits = v.rbits;
+        sa.rbits_base = v.rbits_base;
         sa.geom = ix->d_geom.p;
         sa.units = ws.units.p;
         sa.probe_qr = ws.probe_qr.p;
@@ -1566,6 +1658,7 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         sa.max_dist = R.P.max_dist;
         sa.hdr = R.hdr;
         sa.L = ws.scan_layout;
+        if (staged) ISSL_CUDA(cudaStreamWaitEvent(st, ws.win_ready[wb], 0));
         if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[2 + 2 * w], st));
         switch (ws.scan_rw) {
             case 12: k_scan<12><<<ws.scan_blocks, kScanWarps * 32, ws.scan_smem, st>>>(sa); break;
@@ -1579,6 +1672,7 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, d_n, n, ws.scan32.p, &C->hit_total,
                                      st);
         k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, ws.qhits.p, ws.qhoff.p, v, R.qsig, ws.seg.p);
+        if (staged) ISSL_CUDA(cudaEventRecord(ws.win_free[wb], st));  // the last reader of the window
         k += 7;
         ScoreArgs a;
         a.ix = v;
@@ -1669,6 +1763,7 @@ void fill_stats(const Workspace& ws, float scan_ms, float total_ms, uint64_t lau
     s.launches = launches;
     for (int i = 0; i < 3; i++) s.class_probes[i] = ws.last.class_probes[i];
     s.candidates = ws.last.cands;
+    s.staged_bytes = ws.staged;
 }
 
 issl_score_stats run_stats(issl_index* ix, Workspace& ws) {
@@ -1698,6 +1793,7 @@ void add_stats(issl_score_stats& a, const issl_score_stats& b) {
     a.launches += b.launches;
     for (int i = 0; i < 3; i++) a.class_probes[i] += b.class_probes[i];
     a.candidates += b.candidates;
+    a.staged_bytes += b.staged_bytes;
 }
 
 // One pipeline run over n guides, growing the workspace and rerunning on overflow.
@@ -2044,6 +2140,43 @@ int issl_index_trim(issl_index* ix) {
         ISSL_CUDA(cudaSetDevice(ix->device));
         if (ix->ws) ISSL_CUDA(cudaStreamSynchronize(ix->ws->own_stream));
         ix->ws.reset();
+    });
+}
+
+int issl_index_set_list_placement(issl_index* ix, uint32_t window_slices) {
+    return guarded([&] {
+        ISSL_REQUIRE(ix, ISSL_ERR_ARG, "issl_index_set_list_placement: null argument");
+        ISSL_REQUIRE(window_slices <= static_cast<uint32_t>(issl::kMaxSlices), ISSL_ERR_ARG,
+                     "issl_index_set_list_placement: window_slices must be 0..64");
+        ISSL_CUDA(cudaSetDevice(ix->device));
+        ISSL_CUDA(cudaDeviceSynchronize());  // nothing may be reading the lists while they move
+        const uint64_t idw = ix->n_slices * ix->n_sites * ix->entry_words, rw = issl::rbits_words(ix);
+        if (window_slices && !ix->host_lists) {
+            ix->h_ids.reserve(idw);
+            ix->h_rbits.reserve(rw);
+            ISSL_CUDA(cudaMemcpy(ix->h_ids.p, ix->ids.p, idw * 4, cudaMemcpyDeviceToHost));
+            ISSL_CUDA(cudaMemcpy(ix->h_rbits.p, ix->rbits.p, rw * 4, cudaMemcpyDeviceToHost));
+            ix->ids.release();
+            ix->rbits.release();
+            ix->host_lists = true;
+        } else if (!window_slices && ix->host_lists) {
+            try {
+                ix->ids.reserve(idw);
+                ix->rbits.reserve(rw);
+            } catch (...) {
+                ix->ids.release();
+                ix->rbits.release();
+                throw;
+            }
+            ISSL_CUDA(cudaMemcpy(ix->ids.p, ix->h_ids.p, idw * 4, cudaMemcpyHostToDevice));
+            ISSL_CUDA(cudaMemcpy(ix->rbits.p, ix->h_rbits.p, rw * 4, cudaMemcpyHostToDevice));
+            ix->h_ids.release();
+            ix->h_rbits.release();
+            ix->host_lists = false;
+        }
+        ix->window_slices = window_slices;
+        ix->ws.reset();
+        ix->tuning_version++;  // batch contexts and server slots re-capture their graphs
     });
 }
 
@@ -2409,6 +2542,8 @@ extern "C" int issl_score_device_static(issl_index* ix, const uint64_t* d_sigs, 
                                         uint64_t* d_count, void* stream) {
     return issl::guarded([&] {
         ISSL_REQUIRE(ix && (d_sigs || n == 0) && d_code, ISSL_ERR_ARG, "issl_score_device_static: null argument");
+        ISSL_REQUIRE(!ix->host_lists, ISSL_ERR_UNSUPPORTED,
+                     "issl_score_device_static: the index keeps its lists in host memory (issl_open_mapped)");
         ISSL_REQUIRE(n <= ISSL_STATIC_MAX_GUIDES, ISSL_ERR_ARG,
                      "issl_score_device_static: at most " + std::to_string(ISSL_STATIC_MAX_GUIDES) +
                          " guides per call");

@@ -64,6 +64,15 @@ class Index:
         return cls(h.value)
 
     @classmethod
+    def open_mapped(cls, path: str, device: int = 0, window_slices: int = 4) -> "Index":
+        """An index whose lists stay in page-locked host memory, for indexes larger than HBM
+        (the reference's memory-mapped module): every scoring call streams them to the device
+        window_slices slices at a time. Results are identical to Index.open."""
+        h = C.c_void_p()
+        check(lib().issl_open_mapped(path.encode(), device, window_slices, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
     def from_arrays(cls, sigs, slice_masks, list_sizes, lists, seq_len: int = 20, device: int = 0) -> "Index":
         arrs = [np.ascontiguousarray(a, dtype=np.uint64) for a in (sigs, slice_masks, list_sizes, lists)]
         h = C.c_void_p()
@@ -145,6 +154,11 @@ class Index:
 
     def save(self, path: str) -> None:
         check(lib().issl_save(self._h, path.encode()))
+
+    def set_list_placement(self, window_slices: int) -> None:
+        """window_slices > 0: move the lists to page-locked host memory, streamed per call that
+        many slices at a time; 0: back to HBM. The index must be idle."""
+        check(lib().issl_index_set_list_placement(self._h, window_slices))
 
     def trim(self) -> None:
         """Frees the index's own scoring workspace (re-created by the next scoring call)."""

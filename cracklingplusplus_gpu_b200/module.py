@@ -34,8 +34,8 @@ class GuideResults:
 @dataclass
 class CracklingConfig:
     """The cracklingConfig fields the module uses: input.offtargetSites, offTarget.{enabled,
-    method, scoreThreshold}, general.optimisation, consensus.n (threads/pageLen/memoryMapped are
-    accepted and unused: the index is resident in HBM)."""
+    method, scoreThreshold, memoryMapped}, general.optimisation, consensus.n (threads/pageLen are
+    accepted and unused). memoryMapped keeps the lists in host memory (Index.open_mapped)."""
     offtargetSites: str
     method: str = "mitAndCfd"
     scoreThreshold: float = 75.0
@@ -43,6 +43,7 @@ class CracklingConfig:
     optimisation: str = "ultralow"
     consensusN: int = 0
     threads: int = 0
+    memoryMapped: bool = False
     extra: dict = field(default_factory=dict)
 
 
@@ -65,7 +66,8 @@ class ISSLScoringModule:
         code = C.create_string_buffer(bytes(ord(g.passedOffTargetScore[0]) for g in candidateGuides) + b"\0")
         f = C.POINTER(C.c_double)
         check(lib().issl_module_run(cfg.offtargetSites.encode(), OT_METHODS[cfg.method], cfg.scoreThreshold,
-                                    OPTIMISATION[cfg.optimisation], cfg.consensusN, int(cfg.enabled), n, buf, stride,
+                                    OPTIMISATION[cfg.optimisation], cfg.consensusN,
+                                    int(cfg.enabled) | (2 if cfg.memoryMapped else 0), n, buf, stride,
                                     uniq.ctypes.data_as(C.POINTER(C.c_uint8)),
                                     cons.ctypes.data_as(C.POINTER(C.c_int8)), bt2, mit.ctypes.data_as(f),
                                     cfd.ctypes.data_as(f), code))

@@ -56,6 +56,8 @@ typedef struct {
     int entry_bytes;          /* 8: list entries carry the residual code (one read per scored
                                  hit); 4: chosen when HBM is short (a second read for the
                                  signature). ISSL_ENTRY_BYTES=4|8 in the environment forces it */
+    uint64_t host_bytes;      /* page-locked host memory holding the lists (issl_open_mapped) */
+    int window_slices;        /* slices staged on the device at a time (0: lists resident) */
 } issl_index_info;
 
 /* Message for the last failing call on this thread ("" when none). */
@@ -69,6 +71,17 @@ const char* issl_last_error(void);
  * S slice masks, then per slice 4^w list sizes and N (occ<<32 | id) entries).
  * The file is streamed through pinned staging buffers; no full host copy is made. */
 int issl_open(const char* path, int device, issl_index** out);
+
+/* Load a .issl file for an index whose lists do not fit in HBM: replaces the memory-mapped
+ * module (lib/ISSLScoringModuleMMF.cpp:73-128, selected by offTarget.memoryMapped), which scores
+ * straight from a mapping of the file. Signatures, occurrence counts and bucket offsets are
+ * resident on `device`; the list entries and bit-sliced residual codes are built on the device
+ * slice by slice and kept in page-locked host memory. Every scoring call then streams them back
+ * window_slices slices at a time (two device windows: the copy of the next window overlaps the
+ * scan of the current one), so a call moves the whole lists over the host link once and large
+ * guide batches amortise it. Results are identical to a resident index. Everything else works on
+ * such an index except issl_score_device_static (ISSL_ERR_UNSUPPORTED). */
+int issl_open_mapped(const char* path, int device, uint32_t window_slices, issl_index** out);
 
 /* Same, from host arrays already in the file layout (list_sizes concatenated over slices,
  * lists = S*N entries). Used by embedders that hold the index in memory. */
@@ -158,12 +171,20 @@ typedef struct {
     uint64_t launches;          /* kernels this library launched for the call */
     uint64_t class_probes[3];   /* probes into buckets of < 64, 64..4095 and >= 4096 entries */
     uint64_t candidates;        /* candidate slots the scan wrote, before the ownership rule */
+    uint64_t staged_bytes;      /* host-list index: list bytes copied from host memory */
 } issl_score_stats;
 
 /* Frees the device memory of the index's own scoring workspace (the buffers the plain
  * issl_score* calls grow on demand); the next call re-creates it. The index stays resident.
  * No counterpart in the reference. */
 int issl_index_trim(issl_index* index);
+
+/* Moves an open index's list entries and bit-sliced codes between HBM and page-locked host
+ * memory: window_slices > 0 keeps them in host memory and stages that many slices per device
+ * window while scoring (what issl_open_mapped gives), 0 brings them back to HBM. The index must
+ * be idle (no call on it, its batch contexts or its server in flight); batch contexts and
+ * servers re-capture their graphs on their next call. No counterpart in the reference. */
+int issl_index_set_list_placement(issl_index* index, uint32_t window_slices);
 
 /* Modelled device bytes of one scoring workspace (the per-call buffers of issl_score*,
  * a batch context or a server slot) holding n guides, when the scan finds `candidates_per_guide`

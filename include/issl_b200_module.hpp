@@ -42,7 +42,8 @@ struct inputConfig {
 };
 struct offTargetConfig {  // include/util.hpp:64-72
     bool enabled = true;
-    bool memoryMapped = false;  // accepted, unused: the index is resident in HBM
+    bool memoryMapped = false;  // true: the lists stay in host memory (issl_open_mapped) and are
+                                // streamed per call, for indexes larger than HBM
     otScoreMethod method = mitAndCfd;
     uint8_t threads = 0;        // accepted, unused: the GPU replaces the OpenMP team
     uint64_t pageLen = 0;
@@ -85,10 +86,13 @@ extern "C" {
 // C entry used by language bindings to drive ISSLScoringModule::run on a guide batch:
 // per guide the 20+ character sequence (at seqs + i*stride), isUnique, consensusCount and
 // passedBowtie2 in; mitOfftargetscore, cfdOfftargetscore and passedOffTargetScore in/out (guides
-// the filter skips keep the values passed in, as run() leaves them untouched). Returns ISSL_OK or
-// an ISSL_ERR_* code.
+// the filter skips keep the values passed in, as run() leaves them untouched). flags:
+// ISSL_MODULE_ENABLED (offTarget.enabled), ISSL_MODULE_MEMORY_MAPPED (offTarget.memoryMapped).
+// Returns ISSL_OK or an ISSL_ERR_* code.
+#define ISSL_MODULE_ENABLED 1
+#define ISSL_MODULE_MEMORY_MAPPED 2
 int issl_module_run(const char* index_path, int method, double threshold, int optimisation, int consensus_n,
-                    int enabled, size_t n, const char* seqs, size_t stride, const uint8_t* is_unique,
+                    int flags, size_t n, const char* seqs, size_t stride, const uint8_t* is_unique,
                     const int8_t* consensus_count, const char* passed_bowtie2, double* mit_out, double* cfd_out,
                     char* code_out);
 // Drops every index the module keeps resident (process-lifetime cache keyed by path).
