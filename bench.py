@@ -74,6 +74,7 @@ def parse():
                          "capacity (500M sites, slice-8-28), mapped (lists in host memory) and extract "
                          "(off-target extraction), comma-separated, one JSON line each")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the served-load run")
+    ap.add_argument("--ref-cases", default=None, help="--impl reference --form gpu: cases to run (c0,c1)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="request arrivals per second (Poisson)")
     return ap.parse_args()
 
@@ -406,6 +407,95 @@ def run_reference(args):
                                    f"index; the reference's own 'ISSL scoring time'"},
         "e2e": {"value": value, "unit": "guides/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+# The reference's own GPU scorer (ISSLScoreOfftargets/main_cuda.cpp + issl_cuda.cu, built unchanged
+# for sm_100a into oracle/_ref/issl_cuda_ref) on the small case and on the headline workload.
+REF_GPU_CASES = {
+    "c0": {"workload": "1M-site slice-4-5 index, 1,000 guides (500 copied with 0-4 substitutions and inserted "
+                       "into the site set, 500 random), MIT+CFD 'and', threshold 75",
+           "n_sites": 1_000_000, "slice_config": "slice-4-5", "n_queries": 1000, "seed": 1234, "planted": True},
+    "c1": {"workload": WORKLOAD["workload"], "n_sites": WORKLOAD["n_sites"], "slice_config": WORKLOAD["slice_config"],
+           "n_queries": WORKLOAD["n_queries"], "seed": WORKLOAD["seed"], "planted": False},
+}
+REF_GPU_STAGES = ["Encode (GPU)", "Distance scan (GPU)", "Dedup (GPU)", "MIT LUT (CPU)", "Score (GPU)"]
+
+
+def run_reference_gpu(args):
+    """One JSON line per case: the reference GPU scorer's own stage timings (its stderr summary;
+    scoring time = encode + scan + dedup + MIT LUT + score, index load and output excluded), its
+    results against this library's on the same index and guides, and this library's time."""
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    binary = os.path.join(REPO, "oracle", "_ref", "issl_cuda_ref")
+    if not os.path.exists(binary):
+        print(json.dumps({"impl": "reference", "form": "gpu", "unavailable": "oracle/_ref/issl_cuda_ref was not "
+                          "built (needs the reference sources at build time)"}))
+        return
+    import torch
+    import cracklingplusplus_gpu_b200 as pkg
+    from cracklingplusplus_gpu_b200 import build
+    from cracklingplusplus_gpu_b200.index import decode
+    build.build()
+    torch.cuda.set_device(local)
+    cases = [c for c in ("c0", "c1") if c in (args.ref_cases or "c0,c1").split(",")]
+    for name in cases:
+        c = REF_GPU_CASES[name]
+        n_sites = args.sites or c["n_sites"]
+        nq = args.queries or c["n_queries"]
+        spec = pkg.SynthSpec(seed=c["seed"], n_sites=n_sites, slice_config=c["slice_config"], n_queries=nq,
+                             planted_into_sites=c["planted"])
+        ix, q = pkg.Index.synth(spec, device=local)
+        ours = ix.score(q, "and", 75.0, distinct=False)  # warm-up, and the results compared below
+        d_q = torch.from_numpy(np.ascontiguousarray(q).view(np.int64)).cuda()
+        outs = [torch.empty(nq, dtype=torch.float64, device="cuda") for _ in range(2)] + [
+            torch.empty(nq, dtype=torch.uint8, device="cuda"), torch.empty(nq, dtype=torch.int64, device="cuda")]
+        ms = []
+        for _ in range(5):
+            ix.score_device(d_q.data_ptr(), nq, 2, 75.0, 4, *[t.data_ptr() for t in outs])
+            ms.append(ix.last_stats().total_ms)
+        ours_ms = statistics.median(ms)
+        workdir = tempfile.mkdtemp(dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+        try:
+            idx = os.path.join(workdir, "index.issl")
+            ix.save(idx)
+            ix.close()
+            qf = os.path.join(workdir, "queries.txt")
+            with open(qf, "w") as f:
+                f.write("".join(decode(x) + "\n" for x in q))
+            r = subprocess.run([binary, idx, qf, "4", "75", "and", "out.txt"], cwd=workdir, capture_output=True,
+                               text=True)
+            if r.returncode != 0:
+                print(json.dumps({"impl": "reference", "form": "gpu", "case": name,
+                                  "unavailable": f"reference GPU scorer exited {r.returncode}: "
+                                                 f"{r.stderr.strip()[-200:]}"}), flush=True)
+                continue
+            stage = {k: float(re.search(re.escape(k) + r" time: ([0-9]+) ms", r.stderr).group(1))
+                     for k in REF_GPU_STAGES + ["Loading", "Total execution"]}
+            rows = [ln.split("\t") for ln in open(os.path.join(workdir, "out.txt")).read().splitlines() if ln]
+        finally:
+            shutil.rmtree(workdir, ignore_errors=True)
+        ref_mit = np.array([float(x[1]) for x in rows])
+        ref_cfd = np.array([float(x[2]) for x in rows])
+        ref_cnt = np.array([int(x[3]) for x in rows], dtype=np.uint64)
+        # the reference prints %f: agreement to its 6 decimals
+        same = (np.abs(ref_mit - np.round(ours.mit, 6)) <= 1.5e-6) & (np.abs(ref_cfd - np.round(ours.cfd, 6)) <= 1.5e-6) \
+            & (ref_cnt == ours.count)
+        scoring_ms = sum(stage[k] for k in REF_GPU_STAGES)
+        print(json.dumps({
+            "impl": "reference", "form": "gpu", "case": name,
+            "metric": "guides/sec, the reference's own GPU scorer (issl_cuda.cu) on 1 B200",
+            "value": nq / (scoring_ms / 1e3) if scoring_ms > 0 else None, "unit": "guides/s",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded)",
+            "config": dict(c, n_sites=n_sites, n_queries=nq),
+            "stages_ms": stage, "scoring_ms": scoring_ms,
+            "ours": {"value": nq / (ours_ms / 1e3), "device_ms": ours_ms},
+            "agreement": {"guides": int(nq), "equal_to_6_decimals": int(same.sum()),
+                          "max_abs_mit": float(np.max(np.abs(ref_mit - ours.mit))),
+                          "max_abs_cfd": float(np.max(np.abs(ref_cfd - ours.cfd))),
+                          "counts_equal": int((ref_cnt == ours.count).sum())},
+        }), flush=True)
 
 
 # ---- batched and served forms (300M-site slice-10-37 index) -----------------------------------
@@ -921,7 +1011,10 @@ def main():
     args = parse()
     forms = [f.strip() for f in args.form.split(",") if f.strip()]
     if args.impl == "reference":
-        run_reference(args)
+        if forms == ["gpu"]:
+            run_reference_gpu(args)
+        else:
+            run_reference(args)
     elif forms == ["plain"]:
         run_ours(args)
     else:

@@ -135,7 +135,8 @@ std::vector<std::string> expand_inputs(const char* const* inputs, size_t n) {
 
 // ---- device: matches -> keys ----------------------------------------------------------------
 // Tiles of kTile positions, one 32-position word per thread. The block first packs the tile's
-// bases (and the word after it, which the last windows reach into) into shared memory: per word,
+// bases into shared memory, one word per thread, the last thread packing the word after the tile
+// (which the last windows reach into) and testing none: per word,
 // the 2-bit codes (A C G T -> 0 1 2 3, base j at bits 2j) and three bit planes with one bit per
 // position: valid (the byte is A, C, G or T), lo and hi (the code's two bits). Each thread then
 // tests its 32 positions at once with shifts of the planes of its word and the next:
@@ -146,8 +147,7 @@ std::vector<std::string> expand_inputs(const char* const* inputs, size_t n) {
 //   forward  codes k..k+19, the first most significant (a 2-bit-group reversal of the window)
 //   reverse  the reverse complement of codes k+3..k+22: code k+22-j complemented (x ^ 3) as base
 //            j, which is the window's codes k+3..k+22 in place, complemented
-constexpr uint32_t kTileThreads = 256, kTile = kTileThreads * 32;
-constexpr uint32_t kTileWords = kTileThreads + 1;
+constexpr uint32_t kTileThreads = 256, kTileWords = kTileThreads, kTile = (kTileWords - 1) * 32;
 constexpr uint64_t kSeqPad = kTile + 64;  // zero bytes after the sequences: every tile read is in bounds
 constexpr uint64_t kMask40 = (1ull << 40) - 1;
 
@@ -222,8 +222,8 @@ __global__ void __launch_bounds__(kTileThreads) k_pam_tiles(const uint8_t* __res
         pack_tile(s, tile * kTile, t);
         __syncthreads();
         // positions at or past the end read the zero padding: never bases, never a match
-        uint32_t fwd, rev;
-        match_word(t, threadIdx.x, fwd, rev);
+        uint32_t fwd = 0, rev = 0;
+        if (threadIdx.x + 1 < kTileWords) match_word(t, threadIdx.x, fwd, rev);
         const uint32_t mine = __popc(fwd) + __popc(rev);
         uint32_t incl = mine;
 #pragma unroll

@@ -145,7 +145,7 @@ __host__ __device__ inline WarpLayout warp_layout(uint32_t max_wpb, uint32_t sta
     L.stage_words = (32u * max_wpb + 3u + 3u) & ~3u;  // 32 blocks + alignment slack, 16-byte multiple
     L.qr_off = stages * L.stage_words * 4u;                 // 16-byte aligned (stage_words % 4 == 0)
     L.qm_off = L.qr_off + stages * kStageQr * 8u;
-    L.meta_off = L.qm_off + 32u * 4u;
+    L.meta_off = L.qm_off + 64u * 4u;  // two 32-word guide-mask buffers
     L.bar_off = L.meta_off + stages * static_cast<uint32_t>(sizeof(StageMeta));
     L.bytes = (L.bar_off + stages * 8u + 15u) & ~15u;
     return L;
@@ -473,19 +473,31 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
     const uint32_t* blk = rb + m.delta + lane * wpb;
 #pragma unroll
     for (int j = 0; j < NW; j++) d[j] = blk[j];
-    const uint4* qm4 = reinterpret_cast<const uint4*>(qm);
+    // guide bit j spread to a word (qm[j] = 0 or ~0), double-buffered: the next guide's masks are
+    // written while this guide's are read, one warp barrier per guide
+    if (m.qn) {
+        const uint32_t rq0 = static_cast<uint32_t>(qr[m.qoff] >> 32);
+        __syncwarp();
+        if (lane < NW) qm[lane] = 0u - ((rq0 >> lane) & 1u);
+        __syncwarp();
+    }
     for (uint32_t k = 0; k < m.qn; k++) {
         const uint64_t g = qr[m.qoff + k];
-        const uint32_t rq = static_cast<uint32_t>(g >> 32);
-        __syncwarp();
-        if (lane < NW) qm[lane] = 0u - ((rq >> lane) & 1u);  // guide bit j spread to a word
-        __syncwarp();
-        // mismatch word of each residual position: guide masks come as 128-bit broadcast reads,
-        // two positions per read
+        // guide masks come as 128-bit broadcast reads, two positions per read
+        const uint4* qm4 = reinterpret_cast<const uint4*>(qm + 32u * (k & 1u));
+        uint4 wv[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) wv[v] = qm4[v];
+        if (k + 1 < m.qn) {
+            const uint32_t rqn = static_cast<uint32_t>(qr[m.qoff + k + 1] >> 32);
+            if (lane < NW) qm[32u * ((k + 1) & 1u) + lane] = 0u - ((rqn >> lane) & 1u);
+        }
+        __syncwarp();  // the other buffer is complete; this one's reads are done
+        // mismatch word of each residual position
         uint32_t mm[RW];
 #pragma unroll
         for (int v = 0; v < NV; v++) {
-            const uint4 w = qm4[v];
+            const uint4 w = wv[v];
             if (2 * v < RW) mm[2 * v] = (d[4 * v] ^ w.x) | (d[4 * v + 1] ^ w.y);
             if (2 * v + 1 < RW) mm[2 * v + 1] = (d[4 * v + 2] ^ w.z) | (d[4 * v + 3] ^ w.w);
         }
