@@ -162,6 +162,8 @@ struct __align__(32) HitRec {
     uint64_t sig;
     uint64_t spare;
 };
+// device bytes per candidate slot: the candidate record and the grouped-hit record it may become
+constexpr size_t kCandSlotBytes = sizeof(uint4) + sizeof(HitRec);
 
 struct issl::Workspace {
     int device = 0;
@@ -1073,33 +1075,64 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
         __syncwarp();
         for (uint32_t i = lane; i < L; i += 32) W.idx[atomicAdd(&W.cur[seg[i].r.y], 1u)] = static_cast<uint16_t>(i);
         __syncwarp();
+        // The hits in slice order, 32 at a time, with running exact totals (inclusive warp scans
+        // plus the carry of the earlier chunks). At the last hit of each slice the test is
+        // evaluated on the totals of whole slices; the first slice where it fires is the one the
+        // reference stops in (the totals only grow, so the test fires at every later slice end
+        // too). bm/bc/bn: the totals at the end of the last slice that completed without firing.
+        Fx cm = rm, cc = rc, bm = rm, bc = rc;
+        uint64_t cn = rn, bn = rn;
+        int exit_sl = -1;
+        for (uint32_t c0 = 0; c0 < L && exit_sl < 0; c0 += 32) {
+            const uint32_t t = c0 + lane;
+            FxContribution c{{0, 0}, {0, 0}, 0};
+            uint32_t sl = 0xFFFFFFFFu;
+            if (t < L) {
+                const HitRec hr = seg[W.idx[t]];
+                sl = hr.r.y;
+                c = fx_contribution(P, T, q, hr.r, hr.sig);
+            }
+            uint32_t nsl = __shfl_down_sync(0xffffffffu, sl, 1);
+            if (lane == 31) nsl = t + 1 < L ? seg[W.idx[t + 1]].r.y : 0xFFFFFFFFu;
+            const bool end = t < L && nsl != sl;
+            const Fx im = fx_add(fx_warp_incl(c.mit, lane), cm);
+            const Fx ic = fx_add(fx_warp_incl(c.cfd, lane), cc);
+            const uint64_t in = warp_incl_sum_u64(c.occ, lane) + cn;
+            const bool fire = end && exit_test(P, fx_double(im), fx_double(ic));
+            const unsigned ends = __ballot_sync(0xffffffffu, end), fires = __ballot_sync(0xffffffffu, fire);
+            const unsigned done = fires ? ends & ((1u << (__ffs(fires) - 1)) - 1u) : ends;  // ends before the first fire
+            if (done) {
+                const int e = 31 - __clz(done);
+                bm = Fx{__shfl_sync(0xffffffffu, im.hi, e), __shfl_sync(0xffffffffu, im.lo, e)};
+                bc = Fx{__shfl_sync(0xffffffffu, ic.hi, e), __shfl_sync(0xffffffffu, ic.lo, e)};
+                bn = __shfl_sync(0xffffffffu, in, e);
+            }
+            if (fires) exit_sl = static_cast<int>(__shfl_sync(0xffffffffu, sl, __ffs(fires) - 1));
+            cm = Fx{__shfl_sync(0xffffffffu, im.hi, 31), __shfl_sync(0xffffffffu, im.lo, 31)};
+            cc = Fx{__shfl_sync(0xffffffffu, ic.hi, 31), __shfl_sync(0xffffffffu, ic.lo, 31)};
+            cn = __shfl_sync(0xffffffffu, in, 31);
+        }
+        if (exit_sl < 0) {  // the totals did not fire after all: every hit counts
+            if (P.want_distinct)
+                for (uint32_t j = lane; j < L; j += 32) {
+                    const uint32_t id = seg[j].r.z;
+                    atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                }
+            if (lane == 0) finalise(P, fx_double(cm), fx_double(cc), cn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+            __syncwarp();
+            continue;
+        }
+        const uint32_t b0 = W.cnt[exit_sl], ns = W.cnt[exit_sl + 1] - b0;
+        if (P.want_distinct)  // the sites of the slices before the exit slice
+            for (uint32_t j = lane; j < b0; j += 32) {
+                const uint32_t id = seg[W.idx[j]].r.z;
+                atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+            }
+        rm = bm;
+        rc = bc;
+        rn = bn;
         bool stopped = false;
-        for (uint32_t sl = 0; sl < S && !stopped; sl++) {
-            const uint32_t b0 = W.cnt[sl], ns = W.cnt[sl + 1] - b0;
-            if (!ns) continue;
-            Fx tm{0, 0}, tc{0, 0};
-            uint64_t tn = 0;
-            for (uint32_t j = lane; j < ns; j += 32) {
-                const HitRec hr = seg[W.idx[b0 + j]];
-                const FxContribution c = fx_contribution(P, T, q, hr.r, hr.sig);
-                tm = fx_add(tm, c.mit);
-                tc = fx_add(tc, c.cfd);
-                tn += c.occ;
-            }
-            tm = fx_add(fx_warp_sum(tm), rm);
-            tc = fx_add(fx_warp_sum(tc), rc);
-            for (int d = 16; d > 0; d >>= 1) tn += __shfl_xor_sync(0xffffffffu, tn, d);
-            if (!exit_test(P, fx_double(tm), fx_double(tc))) {
-                if (P.want_distinct)
-                    for (uint32_t j = lane; j < ns; j += 32) {
-                        const uint32_t id = seg[W.idx[b0 + j]].r.z;
-                        atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
-                    }
-                rm = tm;
-                rc = tc;
-                rn += tn;
-                continue;
-            }
+        {
             // the test fires inside this slice: order its hits by list position
             uint32_t P2 = 1;
             while (P2 < ns) P2 <<= 1;
@@ -1513,13 +1546,13 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
 }  // namespace
 
 // The allocations of ensure_capacity as a formula: a fixed part, bytes per guide and bytes per
-// candidate slot (candidate record, grouped hit record, grouped hit signature).
+// candidate slot (candidate record, grouped hit record).
 void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide, uint64_t* per_candidate) {
     const uint64_t S = ix->n_slices, G = ix->n_buckets;
     uint32_t min_chunk = kChunk;
     for (uint32_t c : ix->tuning.chunk) min_chunk = std::min(min_chunk, c);
     const uint64_t slab_slack = 148ull * 16 * kScanWarps * kCandSlab;  // one slab per scan warp, at most
-    *per_candidate = sizeof(uint4) + sizeof(HitRec);
+    *per_candidate = kCandSlotBytes;
     *fixed = 8 * (G + 1) + sizeof(Tables) + sizeof(Counters) + (kScanBlocks + 4) * 12 + 4096 * sizeof(UnitDesc) +
              (65536 + slab_slack) * *per_candidate;
     // qsig, probe lists, hit counts and offsets, exit queues, outputs, set map, wave lists and
@@ -1838,7 +1871,7 @@ void learn_density(Workspace& ws, uint64_t k) { learn_density(ws, k, static_cast
 uint64_t shrunk_chunk(Workspace& ws, uint64_t k) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    const double per_slot = sizeof(uint4) * 2 + sizeof(uint64_t);  // candidate, grouped hit, signature
+    const double per_slot = kCandSlotBytes;
     const double afford = 0.75 * static_cast<double>(free_b) / per_slot;
     const double demand = static_cast<double>(std::max<uint64_t>(ws.last.max_cand, 1));
     learn_density(ws, k, demand);  // size the next run from what this one needed
@@ -1861,7 +1894,7 @@ uint64_t initial_chunk(const Workspace& ws, uint64_t n) {
     if (need <= static_cast<double>(ws.cand_cap)) return c;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-        const double per_slot = sizeof(uint4) * 2 + sizeof(uint64_t);
+        const double per_slot = kCandSlotBytes;
         const double afford = 0.75 * static_cast<double>(free_b) / per_slot + static_cast<double>(ws.cand_cap);
         const double fit = afford / (ws.cand_density * 1.1);
         if (fit < static_cast<double>(c)) c = std::max<uint64_t>(static_cast<uint64_t>(fit), 1);
