@@ -16,6 +16,8 @@
 // either prints the sorted lines or run-length counts them into (signature, occurrences) pairs
 // that build the resident index directly.
 #include <cuda_runtime.h>
+#include <fcntl.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cctype>
@@ -24,6 +26,7 @@
 #include <filesystem>
 #include <fstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "issl_internal.cuh"
@@ -69,10 +72,24 @@ char append_trimmed(const char* b, const char* e, bool fasta, std::string& out) 
     return first;
 }
 
+// Whole lines [p, end) of one input: FASTA header lines become kSep (a new record), sequence
+// lines are appended trimmed and upper-cased (their record's lines concatenate); in a plain file
+// every line is followed by kSep. Lines end at '\n' as std::getline ends them.
+void parse_lines(const char* p, const char* end, bool fasta, std::string& out) {
+    while (p < end) {
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', static_cast<size_t>(end - p)));
+        const char* e = nl ? nl : end;
+        const char first = append_trimmed(p, e, fasta, out);
+        if (!fasta || first == '>') out.push_back(static_cast<char>(kSep));
+        p = nl ? nl + 1 : end;
+    }
+}
+
 // Appends the sequences of one input file to `out`, each followed by kSep (:66-104): a file whose
-// first line starts with '>' is FASTA (records start at header lines, their lines concatenated);
-// anything else holds one sequence per line. One pass over the file's bytes; lines end at '\n'
-// as std::getline ends them.
+// first line starts with '>' is FASTA (records start at header lines, their lines concatenated;
+// the first header is skipped); anything else holds one sequence per line. Large files are cut
+// at line starts into one piece per host thread; the pieces are parsed in parallel and joined in
+// order, which gives exactly the sequential result (a piece's output depends only on its lines).
 void append_sequences(const std::string& path, std::string& out) {
     FILE* fp = std::fopen(path.c_str(), "rb");
     ISSL_REQUIRE(fp, ISSL_ERR_IO, "cannot open input " + path);
@@ -87,29 +104,56 @@ void append_sequences(const std::string& path, std::string& out) {
         ISSL_REQUIRE(got == buf.size(), ISSL_ERR_IO, "short read of " + path);
     }
     if (buf.empty()) return;
-    out.reserve(out.size() + buf.size() + 16);
     const char* p = buf.data();
     const char* end = p + buf.size();
-    auto next_line = [&](const char*& b, const char*& e) -> bool {
-        if (p >= end) return false;
-        b = p;
-        const char* nl = static_cast<const char*>(std::memchr(p, '\n', static_cast<size_t>(end - p)));
-        e = nl ? nl : end;
+    const bool fasta = *p == '>';  // the raw first line starts with '>'
+    if (fasta) {
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', buf.size()));
         p = nl ? nl + 1 : end;
-        return true;
-    };
-    const char *b, *e;
-    next_line(b, e);
-    if (b < e && *b == '>') {  // FASTA: the raw first line starts with '>' (the header is skipped)
-        while (next_line(b, e))
-            if (append_trimmed(b, e, true, out) == '>') out.push_back(static_cast<char>(kSep));
-        out.push_back(static_cast<char>(kSep));
-    } else {
-        do {
-            append_trimmed(b, e, false, out);
-            out.push_back(static_cast<char>(kSep));
-        } while (next_line(b, e));
     }
+    const size_t bytes = static_cast<size_t>(end - p);
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const unsigned T = bytes >= (8u << 20) ? hw : 1u;
+    std::vector<const char*> cut(T + 1);
+    cut[0] = p;
+    cut[T] = end;
+    for (unsigned t = 1; t < T; t++) {  // piece t starts at the first line start at or after its share
+        const char* c = std::max(cut[t - 1], p + bytes / T * t);
+        if (c > p && c < end && c[-1] != '\n') {
+            const char* nl = static_cast<const char*>(std::memchr(c, '\n', static_cast<size_t>(end - c)));
+            c = nl ? nl + 1 : end;
+        }
+        cut[t] = c;
+    }
+    std::vector<std::string> part(T);
+    if (T == 1) {
+        parse_lines(cut[0], cut[1], fasta, part[0]);
+    } else {
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < T; t++)
+            pool.emplace_back([&, t] {
+                part[t].reserve(static_cast<size_t>(cut[t + 1] - cut[t]) + 16);
+                parse_lines(cut[t], cut[t + 1], fasta, part[t]);
+            });
+        for (auto& th : pool) th.join();
+    }
+    size_t at = out.size(), total = 0;
+    for (auto& s : part) total += s.size();
+    out.resize(at + total + (fasta ? 1 : 0));
+    std::vector<size_t> off(T);
+    for (unsigned t = 0; t < T; t++) {
+        off[t] = at;
+        at += part[t].size();
+    }
+    if (T == 1) {
+        std::memcpy(&out[off[0]], part[0].data(), part[0].size());
+    } else {
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < T; t++)
+            pool.emplace_back([&, t] { std::memcpy(&out[off[t]], part[t].data(), part[t].size()); });
+        for (auto& th : pool) th.join();
+    }
+    if (fasta) out[at] = static_cast<char>(kSep);  // the last record's end
 }
 
 std::vector<std::string> expand_inputs(const char* const* inputs, size_t n) {
@@ -399,27 +443,65 @@ int issl_extract_offtargets(const char* const* inputs, size_t n_inputs, const ch
         } g{st};
         issl::Extracted x;
         issl::extract_sorted(files, x, st);
-        FILE* fp = std::fopen(out_path, "wb");
-        ISSL_REQUIRE(fp, ISSL_ERR_IO, std::string("cannot write ") + out_path);
+        const int fd = ::open(out_path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+        ISSL_REQUIRE(fd >= 0, ISSL_ERR_IO, std::string("cannot write ") + out_path);
         struct F {
-            FILE* f;
-            ~F() { std::fclose(f); }
-        } ff{fp};
-        // the text, produced on the device in slices of at most 64M lines
-        const uint64_t line = issl::kSiteLen + 1, slab = 64ull << 20;
+            int fd;
+            ~F() { ::close(fd); }
+        } ff{fd};
+        // The text, made on the device in slabs of up to 16M lines and copied into two page-locked
+        // host buffers: slab i+1 is converted and copied while the host threads write slab i at
+        // its file offset.
+        const uint64_t line = issl::kSiteLen + 1, slab = 16ull << 20;
         if (x.n) {
-            issl::DevBuf<char> d_txt;
-            std::vector<char> h_txt;
             const uint64_t lines = std::min<uint64_t>(x.n, slab);
-            d_txt.reserve(lines * line);
-            h_txt.resize(lines * line);
-            for (uint64_t i = 0; i < x.n; i += slab) {
-                const uint64_t k = std::min<uint64_t>(slab, x.n - i);
-                issl::k_keys_to_text<<<issl::grid_for(k), 256, 0, st>>>(x.keys + i, k, d_txt.p);  // 256 keys per block
-                ISSL_CUDA(cudaMemcpyAsync(h_txt.data(), d_txt.p, k * line, cudaMemcpyDeviceToHost, st));
-                ISSL_CUDA(cudaStreamSynchronize(st));
-                ISSL_REQUIRE(std::fwrite(h_txt.data(), 1, k * line, fp) == k * line, ISSL_ERR_IO,
-                             std::string("short write to ") + out_path);
+            issl::DevBuf<char> d_txt[2];
+            issl::PinnedBuf<char> h_txt[2];
+            cudaEvent_t ready[2];
+            for (int b = 0; b < 2; b++) {
+                d_txt[b].reserve(lines * line);
+                h_txt[b].reserve(lines * line);
+                ISSL_CUDA(cudaEventCreateWithFlags(&ready[b], cudaEventDisableTiming));
+            }
+            struct E {
+                cudaEvent_t* e;
+                ~E() {
+                    cudaEventDestroy(e[0]);
+                    cudaEventDestroy(e[1]);
+                }
+            } ee{ready};
+            const uint64_t n_slabs = (x.n + slab - 1) / slab;
+            auto issue = [&](uint64_t i) {
+                const int b = static_cast<int>(i & 1);
+                const uint64_t k = std::min<uint64_t>(slab, x.n - i * slab);
+                issl::k_keys_to_text<<<issl::grid_for(k), 256, 0, st>>>(x.keys + i * slab, k, d_txt[b].p);
+                ISSL_CUDA(cudaMemcpyAsync(h_txt[b].p, d_txt[b].p, k * line, cudaMemcpyDeviceToHost, st));
+                ISSL_CUDA(cudaEventRecord(ready[b], st));
+            };
+            const unsigned T = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+            issue(0);
+            for (uint64_t i = 0; i < n_slabs; i++) {
+                if (i + 1 < n_slabs) issue(i + 1);  // its buffer held slab i-1, already written
+                const int b = static_cast<int>(i & 1);
+                ISSL_CUDA(cudaEventSynchronize(ready[b]));
+                const uint64_t bytes = std::min<uint64_t>(slab, x.n - i * slab) * line, base = i * slab * line;
+                std::vector<std::thread> pool;
+                std::vector<int> ok(T, 1);
+                for (unsigned t = 0; t < T; t++)
+                    pool.emplace_back([&, t] {
+                        uint64_t o = bytes / T * t;
+                        const uint64_t e = t + 1 == T ? bytes : bytes / T * (t + 1);
+                        while (o < e) {
+                            const ssize_t w = ::pwrite(fd, h_txt[b].p + o, e - o, static_cast<off_t>(base + o));
+                            if (w <= 0) {
+                                ok[t] = 0;
+                                return;
+                            }
+                            o += static_cast<uint64_t>(w);
+                        }
+                    });
+                for (auto& th : pool) th.join();
+                for (int v : ok) ISSL_REQUIRE(v, ISSL_ERR_IO, std::string("short write to ") + out_path);
             }
         }
         if (n_offtargets) *n_offtargets = x.n;

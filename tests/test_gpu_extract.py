@@ -51,6 +51,46 @@ def inputs(tmp_path_factory):
     return [str(fa), str(txt), str(sub)]
 
 
+def _big_genome(rng, n):
+    """Like _genome, built with array operations (megabase sizes)."""
+    b = np.frombuffer(b"ACGT", np.uint8)[rng.choice(4, n, p=[0.295, 0.205, 0.205, 0.295])].copy()
+    for _ in range(n // 20000):
+        a, c = rng.integers(0, n - 200, 2)
+        b[c:c + 150] = b[a:a + 150]
+    for _ in range(n // 50000):
+        a = int(rng.integers(0, n - 50))
+        b[a:a + int(rng.integers(1, 40))] = ord("N")
+    for _ in range(n // 80000):
+        a = int(rng.integers(0, n - 300))
+        b[a:a + 300] += 32  # lower case
+    return b.tobytes()
+
+
+def test_large_inputs_parsed_in_pieces(native, tmp_path):
+    """Inputs above 8 MB are cut at line starts and parsed by all host threads: FASTA records
+    with CRLF lines and blank lines inside a record, and a plain file of many lines without a
+    final newline must still give exactly the restatement's output."""
+    rng = np.random.default_rng(23)
+    fa = tmp_path / "big.fa"
+    with open(fa, "wb") as f:
+        for r in range(4):
+            f.write(b">rec%d\r\n" % r)
+            g = _big_genome(rng, 3_000_000 + 100_000 * r)
+            f.write(b"\r\n".join(g[i:i + 70] for i in range(0, len(g), 70)) + b"\r\n")
+            if r == 1:
+                f.write(b"\n  \n")
+    txt = tmp_path / "big.txt"
+    with open(txt, "wb") as f:
+        f.write(b"\n".join(_big_genome(rng, 1000 + (i % 7) * 300) for i in range(7000)))
+    inputs = [str(fa), str(txt)]
+    assert os.path.getsize(fa) > 8 << 20 and os.path.getsize(txt) > 8 << 20
+    out = str(tmp_path / "ot.txt")
+    n = native.extract_offtargets(inputs, out)
+    want = eo.extract_text(inputs)
+    assert n == want.count(b"\n") and n > 100000
+    assert open(out, "rb").read() == want
+
+
 def test_extraction_equals_restatement(native, inputs, tmp_path):
     out = str(tmp_path / "ot.txt")
     n = native.extract_offtargets(inputs, out)
