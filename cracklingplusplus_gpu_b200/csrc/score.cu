@@ -153,14 +153,14 @@ __host__ __device__ inline WarpLayout warp_layout(uint32_t max_wpb, uint32_t sta
 
 }  // namespace issl
 
-// One owned hit grouped under its guide: (list position, slice, site id, occurrences) and the
-// site's signature. 32 bytes, written whole by one thread: hits land in their guide's segment in
-// arrival order, and a scattered write of less than a 32-byte sector costs a DRAM read of the
-// sector when it is evicted partly written.
+// One owned hit grouped under its guide: (list position, slice, site id, occurrences) and its MIT
+// and CFD contributions (each already multiplied by the occurrences; the scorers drop the one the
+// guide's method does not use). 32 bytes, written whole by one thread: hits land in their guide's
+// segment in arrival order, and a scattered write of less than a 32-byte sector costs a DRAM read
+// of the sector when it is evicted partly written.
 struct __align__(32) HitRec {
     uint4 r;
-    uint64_t sig;
-    uint64_t spare;
+    double mit, cfd;
 };
 // device bytes per candidate slot: the candidate record and the grouped-hit record it may become
 constexpr size_t kCandSlotBytes = sizeof(uint4) + sizeof(HitRec);
@@ -181,7 +181,7 @@ struct issl::Workspace {
     size_t ascii_cap = 0;
     DevBuf<uint32_t> probe_gb;
     DevBuf<uint64_t> probe_qr;  // per probe slot: guide | residual << 32 (+2 padding)
-    DevBuf<uint32_t> bucket_cnt, bucket_qstart;
+    DevBuf<uint32_t> bucket_cnt, bucket_qstart, bucket_ustart;
     DevBuf<UnitDesc> units;
     DevBuf<uint4> cands;  // candidate slots
     DevBuf<HitRec> seg;   // owned hits grouped per guide
@@ -316,44 +316,80 @@ struct BucketLoad {
     }
 };
 
+// the bucket's first probe slot and first unit (exclusive prefixes over the wave's buckets)
 struct BucketStore {
-    const uint32_t* cnt;
-    const uint64_t* off;
     uint32_t* qstart;
-    UnitDesc* units;
-    uint64_t unit_cap;
-    uint64_t n_sites;
-    ChunkClasses cc;
+    uint32_t* ustart;
     uint64_t g0;
-    __device__ void operator()(uint64_t gi, uint64_t ex, uint64_t inc) const {
-        const uint64_t g = g0 + gi;
-        qstart[g] = static_cast<uint32_t>(ex);
-        const uint32_t c = static_cast<uint32_t>(inc) - static_cast<uint32_t>(ex);
-        if (!c) return;
-        const uint64_t u0 = ex >> 32, u1 = inc >> 32;
-        const uint32_t s = static_cast<uint32_t>(off[g] / n_sites);
-        const uint64_t e0 = off[g] - s * n_sites, e1 = off[g + 1] - s * n_sites;  // list positions
-        const uint64_t C = chunk_of(e1 - e0, cc);
-        const uint32_t ng = (c + kGroup - 1) / kGroup;
-        uint64_t u = u0;
-        for (uint64_t blk = e0 / C; blk * C < e1 && u < u1; blk++) {
-            const uint64_t cb = blk * C > e0 ? blk * C : e0;
-            const uint64_t ce = (blk + 1) * C < e1 ? (blk + 1) * C : e1;
-            const uint16_t len = static_cast<uint16_t>(ce - cb);
-            for (uint32_t j = 0; j < ng; j++, u++) {
-                if (u >= unit_cap) return;
-                UnitDesc d;
-                d.p0 = static_cast<uint32_t>(cb);
-                d.qbeg = static_cast<uint32_t>(ex) + j * kGroup;
-                d.len = len;
-                d.qn = static_cast<uint8_t>(c - j * kGroup < kGroup ? c - j * kGroup : kGroup);
-                d.s = static_cast<uint8_t>(s);
-                d.pad = 0;
-                units[u] = d;
-            }
-        }
+    __device__ void operator()(uint64_t gi, uint64_t ex, uint64_t) const {
+        qstart[g0 + gi] = static_cast<uint32_t>(ex);
+        ustart[g0 + gi] = static_cast<uint32_t>(ex >> 32);
     }
 };
+
+// Slice of a list position in global entry numbering (s * n + position), without a 64-bit divide:
+// a double estimate, corrected by one either way.
+__device__ __forceinline__ uint64_t slice_of_entry(uint64_t e, uint64_t n, double inv_n) {
+    uint64_t s = static_cast<uint64_t>(static_cast<double>(e) * inv_n);
+    if (s * n > e) s--;
+    else if ((s + 1) * n <= e) s++;
+    return s;
+}
+
+// Unit descriptors, kUnitsPerThread consecutive units per thread. The first unit's bucket is the
+// last bucket of the wave whose first unit is at or before it (binary search of the units'
+// exclusive prefix; empty buckets share their successor's prefix, so the search lands on the
+// bucket that owns the unit); the following units advance from there. A bucket's units run over
+// the chunk-aligned blocks of its list range, and within a block over its groups of up to kGroup
+// guides.
+constexpr uint32_t kUnitsPerThread = 8;
+__global__ void k_expand_units(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off,
+                               const uint32_t* __restrict__ qstart, const uint32_t* __restrict__ ustart, uint64_t g0,
+                               uint64_t nb, uint64_t n_sites, double inv_n, ChunkClasses cc,
+                               const Counters* __restrict__ ctr, UnitDesc* __restrict__ units) {
+    const uint32_t n = ctr->n_units;  // at most the buffer's capacity
+    const uint64_t g_end = g0 + nb;
+    for (uint64_t base = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) * kUnitsPerThread; base < n;
+         base += static_cast<uint64_t>(gridDim.x) * blockDim.x * kUnitsPerThread) {
+        uint64_t lo = 0, hi = nb;  // first bucket whose first unit is after `base`
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (ustart[g0 + mid] <= base) lo = mid + 1;
+            else hi = mid;
+        }
+        uint64_t g = g0 + lo - 1, have = ~0ull;
+        uint32_t c = 0, u0 = 0, lc = 0, ng = 1, q0 = 0;
+        uint64_t s = 0, e0 = 0, e1 = 0;
+        const uint64_t last = base + kUnitsPerThread < n ? base + kUnitsPerThread : n;
+        for (uint64_t u = base; u < last; u++) {
+            while (g + 1 < g_end && ustart[g + 1] <= u) g++;
+            if (g != have) {
+                have = g;
+                c = cnt[g];
+                u0 = ustart[g];
+                q0 = qstart[g];
+                s = slice_of_entry(off[g], n_sites, inv_n);
+                e0 = off[g] - s * n_sites;  // list positions
+                e1 = off[g + 1] - s * n_sites;
+                lc = __ffs(static_cast<uint32_t>(chunk_of(e1 - e0, cc))) - 1;  // unit sizes are powers of 2
+                ng = (c + kGroup - 1) / kGroup;
+            }
+            const uint32_t r = static_cast<uint32_t>(u) - u0;
+            const uint32_t k = r / ng, j = r - k * ng;
+            const uint64_t blk = (e0 >> lc) + k;
+            const uint64_t cb = (blk << lc) > e0 ? (blk << lc) : e0;
+            const uint64_t ce = ((blk + 1) << lc) < e1 ? ((blk + 1) << lc) : e1;
+            UnitDesc d;
+            d.p0 = static_cast<uint32_t>(cb);
+            d.qbeg = q0 + j * kGroup;
+            d.len = static_cast<uint16_t>(ce - cb);
+            d.qn = static_cast<uint8_t>(c - j * kGroup < kGroup ? c - j * kGroup : kGroup);
+            d.s = static_cast<uint8_t>(s);
+            d.pad = 0;
+            units[u] = d;
+        }
+    }
+}
 
 // work counters for the roofline: distinct buckets scanned and entries streamed (a bucket's
 // entries are read once per group of up to kGroup guides)
@@ -742,33 +778,6 @@ struct StoreQoff {
     }
 };
 
-// One thread per owned hit (many independent loads in flight): the list entry gives the site id,
-// its occurrences and (8-byte entries) its residual code, from which the signature is rebuilt;
-// with 4-byte entries the signature is a second read. Written into the guide's segment so that
-// the scorers read only contiguous data.
-__global__ void k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint32_t* __restrict__ qhits,
-                              const uint32_t* __restrict__ qhoff, IndexView ix, const uint64_t* __restrict__ qsig,
-                              HitRec* __restrict__ seg) {
-    __shared__ SliceGeom g[kMaxSlices];
-    for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
-    __syncthreads();
-    if (blockIdx.x == 0 && threadIdx.x == 0) c->hits += c->hit_total;
-    if (c->overflow) return;
-    const uint32_t n = c->n_cand;
-    for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x) {
-        const uint4 r = cands[h];
-        if (r.x == kDeadCand) continue;
-        const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
-        const uint32_t sl = r.x >> kGuideBits;
-        uint32_t id, occ;
-        uint64_t sig;
-        load_site(ix, sl, r.y, qsig[q], g[sl], id, occ, sig);
-        // the decrement leaves qhits all zero for the next call
-        const uint32_t slot = qhoff[q] + atomicSub(&qhits[q], 1u) - 1u;
-        seg[slot] = HitRec{make_uint4(r.y, sl, id, occ), sig, 0ull};
-    }
-}
-
 // ---------------------------------------------------------------------------------------------
 // 7. scoring of one guide's hits in the reference's visiting order
 __device__ __forceinline__ uint64_t order_key(const uint4& r) {
@@ -816,6 +825,40 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
         c.cfd = __dmul_rn(s, static_cast<double>(occ));
     }
     return c;
+}
+
+// One thread per owned hit (many independent loads in flight): the list entry gives the site id,
+// its occurrences and (8-byte entries) its residual code, from which the signature is rebuilt;
+// with 4-byte entries the signature is a second read. The hit's MIT and CFD contributions are
+// computed here, where the random reads leave the arithmetic units idle, and written into the
+// guide's segment so that the scorers read only contiguous data.
+__global__ void k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint32_t* __restrict__ qhits,
+                              const uint32_t* __restrict__ qhoff, IndexView ix, const uint64_t* __restrict__ qsig,
+                              const Tables* __restrict__ tables, HitRec* __restrict__ seg) {
+    __shared__ SliceGeom g[kMaxSlices];
+    for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) c->hits += c->hit_total;
+    if (c->overflow) return;
+    const Tables& T = *tables;
+    ScoreParams both{};
+    both.calc_mit = 1;
+    both.calc_cfd = 1;
+    const uint32_t n = c->n_cand;
+    for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x) {
+        const uint4 r = cands[h];
+        if (r.x == kDeadCand) continue;
+        const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
+        const uint32_t sl = r.x >> kGuideBits;
+        const uint64_t gq = qsig[q];
+        uint32_t id, occ;
+        uint64_t sig;
+        load_site(ix, sl, r.y, gq, g[sl], id, occ, sig);
+        const Contribution ct = contribution(T, both, gq, sig, occ);
+        // the decrement leaves qhits all zero for the next call
+        const uint32_t slot = qhoff[q] + atomicSub(&qhits[q], 1u) - 1u;
+        seg[slot] = HitRec{make_uint4(r.y, sl, id, occ), ct.mit, ct.cfd};
+    }
 }
 
 __device__ __forceinline__ bool exit_test(const ScoreParams& P, double mit, double cfd) {
@@ -953,11 +996,9 @@ struct Acc {
     uint64_t occ;
 };
 
-// r: seg record (position, slice, site id, occurrences), sig: the site's signature
-__device__ __forceinline__ FxContribution fx_contribution(const ScoreParams& P, const Tables& T, uint64_t q,
-                                                         const uint4& r, uint64_t sig) {
-    const Contribution c = contribution(T, P, q, sig, r.w);
-    return FxContribution{fx_from(c.mit), fx_from(c.cfd), c.occ};
+// a grouped hit's contributions under the guide's method (contribution() with its flags)
+__device__ __forceinline__ FxContribution fx_contribution(const ScoreParams& P, const HitRec& h) {
+    return FxContribution{fx_from(P.calc_mit ? h.mit : 0.0), fx_from(P.calc_cfd ? h.cfd : 0.0), h.r.w};
 }
 
 constexpr int kWarpSort = 1024;  // exiting guides with more hits are ordered by a whole block
@@ -968,7 +1009,6 @@ constexpr int kWarpSort = 1024;  // exiting guides with more hits are ordered by
 // test fires go to the ordered scorers.
 __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const Tables& T = *a.tables;
     if (a.counters->overflow) return;  // rerun follows
     const uint64_t gw = blockIdx.x * 8ull + warp, nw = gridDim.x * 8ull;
     const uint64_t n = a.d_nact ? *a.d_nact : guide_count(a.d_n, a.n);
@@ -976,13 +1016,12 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         const uint64_t qi = a.active ? a.active[i] : i;
         const ScoreParams P = params_of(a, qi);
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
-        const uint64_t q = a.qsig[qi];
         const HitRec* seg = a.seg + h0;
         Fx tm{0, 0}, tc{0, 0};
         uint64_t tn = 0;
         for (uint32_t j = lane; j < L; j += 32) {
             const HitRec hr = seg[j];
-            const FxContribution c = fx_contribution(P, T, q, hr.r, hr.sig);
+            const FxContribution c = fx_contribution(P, hr);
             tm = fx_add(tm, c.mit);
             tc = fx_add(tc, c.cfd);
             tn += c.occ;
@@ -1038,7 +1077,6 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
     extern __shared__ __align__(16) uint8_t s_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     OrderedSmem& W = reinterpret_cast<OrderedSmem*>(s_raw)[warp];
-    const Tables& T = *a.tables;
     if (a.counters->overflow) return;  // rerun follows
     const uint32_t S = a.ix.n_slices;
     const uint32_t n_exit = a.counters->n_exit;
@@ -1055,7 +1093,6 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             rn = pr.occ;
         }
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
-        const uint64_t q = a.qsig[qi];
         const HitRec* seg = a.seg + h0;
         // counting sort of the hits by slice
         for (uint32_t t = lane; t <= S; t += 32) W.cnt[t] = 0;
@@ -1090,7 +1127,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             if (t < L) {
                 const HitRec hr = seg[W.idx[t]];
                 sl = hr.r.y;
-                c = fx_contribution(P, T, q, hr.r, hr.sig);
+                c = fx_contribution(P, hr);
             }
             uint32_t nsl = __shfl_down_sync(0xffffffffu, sl, 1);
             if (lane == 31) nsl = t + 1 < L ? seg[W.idx[t + 1]].r.y : 0xFFFFFFFFu;
@@ -1162,7 +1199,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
                 if (t < ns) {
                     const HitRec hr = seg[W.keys[t] & 1023u];
                     id = hr.r.z;
-                    c = fx_contribution(P, T, q, hr.r, hr.sig);
+                    c = fx_contribution(P, hr);
                 }
                 const Fx im = fx_add(fx_warp_incl(c.mit, lane), rm);
                 const Fx ic = fx_add(fx_warp_incl(c.cfd, lane), rc);
@@ -1195,7 +1232,6 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
     __shared__ uint64_t s_wn[8];
     __shared__ int s_first;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const Tables& T = *a.tables;
     if (a.counters->overflow) return;  // rerun follows
     const uint32_t n_big = a.counters->n_big;
     for (uint32_t b = blockIdx.x; b < n_big; b += gridDim.x) {
@@ -1211,7 +1247,6 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
         }
         const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
         HitRec* seg = a.seg + h0;
-        const uint64_t q = a.qsig[qi];
         uint32_t P2 = 1;
         while (P2 < L) P2 <<= 1;
         const bool in_smem = L <= static_cast<uint32_t>(kBlockHits);
@@ -1251,7 +1286,7 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
                 const uint32_t h = in_smem ? static_cast<uint32_t>(s_bkeys[t] & ((1u << kBlockIdxBits) - 1)) : t;
                 const HitRec hr = seg[h];
                 id = hr.r.z;
-                c = fx_contribution(P, T, q, hr.r, hr.sig);
+                c = fx_contribution(P, hr);
             }
             Fx im = fx_warp_incl(c.mit, lane), ic = fx_warp_incl(c.cfd, lane);
             uint64_t in = warp_incl_sum_u64(c.occ, lane);
@@ -1484,6 +1519,7 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
     if (ws.g_cap < G + 1) {
         ws.bucket_cnt.reserve(G + 1);
         ws.bucket_qstart.reserve(G + 1);
+        ws.bucket_ustart.reserve(G + 1);
         ISSL_CUDA(cudaMemsetAsync(ws.bucket_cnt.p, 0, (G + 1) * 4, st));
         ws.g_cap = G + 1;
         ws.epoch++;
@@ -1553,7 +1589,7 @@ void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide,
     for (uint32_t c : ix->tuning.chunk) min_chunk = std::min(min_chunk, c);
     const uint64_t slab_slack = 148ull * 16 * kScanWarps * kCandSlab;  // one slab per scan warp, at most
     *per_candidate = kCandSlotBytes;
-    *fixed = 8 * (G + 1) + sizeof(Tables) + sizeof(Counters) + (kScanBlocks + 4) * 12 + 4096 * sizeof(UnitDesc) +
+    *fixed = 12 * (G + 1) + sizeof(Tables) + sizeof(Counters) + (kScanBlocks + 4) * 12 + 4096 * sizeof(UnitDesc) +
              (65536 + slab_slack) * *per_candidate;
     // qsig, probe lists, hit counts and offsets, exit queues, outputs, set map, wave lists and
     // running totals; scan units
@@ -1682,14 +1718,16 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         const unsigned pgrid = grid_for(n * (s1 - s0), 256, sms * 16);
         k_probe_count<<<pgrid, 256, 0, st>>>(v, R.qsig, wp, ws.probe_gb.p, ws.bucket_cnt.p, off);
         device_scan<uint64_t, OpSum>(BucketLoad{ws.bucket_cnt.p, off, ix->n_sites, cc, g0},
-                                     BucketStore{ws.bucket_cnt.p, off, ws.bucket_qstart.p, ws.units.p, ws.unit_cap,
-                                                 ix->n_sites, cc, g0},
+                                     BucketStore{ws.bucket_qstart.p, ws.bucket_ustart.p, g0},
                                      nullptr, g1 - g0, ws.scan64.p, &C->bucket_total, st);
         k_units_finalize<<<1, 1, 0, st>>>(C, ws.unit_cap);
+        k_expand_units<<<sms * 8, 256, 0, st>>>(ws.bucket_cnt.p, off, ws.bucket_qstart.p, ws.bucket_ustart.p, g0,
+                                                g1 - g0, ix->n_sites, 1.0 / static_cast<double>(ix->n_sites), cc, C,
+                                                ws.units.p);
         k_bucket_stats<<<sms * 4, 256, 0, st>>>(ws.bucket_cnt.p, off, g0, g1, ix->d_geom.p, ix->n_sites, C);
         k_probe_scatter<<<pgrid, 256, 0, st>>>(v, R.qsig, wp, ws.probe_gb.p, ws.bucket_cnt.p, ws.bucket_qstart.p,
                                                ws.probe_qr.p);
-        k += 7;
+        k += 8;
         ScanArgs sa;
         sa.rbits = v.rbits;
         sa.rbits_base = v.rbits_base;
@@ -1716,7 +1754,8 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, v, ws.qhits.p, R.sets, qset);
         device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, d_n, n, ws.scan32.p, &C->hit_total,
                                      st);
-        k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, ws.qhits.p, ws.qhoff.p, v, R.qsig, ws.seg.p);
+        k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, ws.qhits.p, ws.qhoff.p, v, R.qsig, ws.tables.p,
+                                               ws.seg.p);
         if (staged) ISSL_CUDA(cudaEventRecord(ws.win_free[wb], st));  // the last reader of the window
         k += 7;
         ScoreArgs a;
@@ -2386,7 +2425,6 @@ template <int RW>
 __device__ __forceinline__ void static_block(const StaticArgs& a, const SliceGeom* geom, uint32_t s, uint64_t b,
                                              uint32_t e0, uint32_t e1, const uint32_t* qm, uint4* hits,
                                              uint32_t* cnt) {
-    constexpr int NW = 2 * RW;
     const SliceGeom& g = geom[s];
     const uint32_t* blk = a.ix.rbits + g.wbase + b * g.wpb;
     uint32_t mm[RW];
