@@ -336,58 +336,42 @@ __device__ __forceinline__ uint64_t slice_of_entry(uint64_t e, uint64_t n, doubl
     return s;
 }
 
-// Unit descriptors, kUnitsPerThread consecutive units per thread. The first unit's bucket is the
-// last bucket of the wave whose first unit is at or before it (binary search of the units'
-// exclusive prefix; empty buckets share their successor's prefix, so the search lands on the
-// bucket that owns the unit); the following units advance from there. A bucket's units run over
-// the chunk-aligned blocks of its list range, and within a block over its groups of up to kGroup
-// guides.
-constexpr uint32_t kUnitsPerThread = 8;
+// Unit descriptors, one thread per unit. The unit's bucket is the last bucket of the wave whose
+// first unit is at or before it (binary search of the units' exclusive prefix; empty buckets share
+// their successor's prefix, so the search lands on the bucket that owns the unit). A bucket's
+// units run over the chunk-aligned blocks of its list range, and within a block over its groups
+// of up to kGroup guides. (Walking forward from one search to the next units instead is no faster
+// on dense waves and crawls over the empty buckets of sparse ones.)
 __global__ void k_expand_units(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off,
                                const uint32_t* __restrict__ qstart, const uint32_t* __restrict__ ustart, uint64_t g0,
                                uint64_t nb, uint64_t n_sites, double inv_n, ChunkClasses cc,
                                const Counters* __restrict__ ctr, UnitDesc* __restrict__ units) {
     const uint32_t n = ctr->n_units;  // at most the buffer's capacity
-    const uint64_t g_end = g0 + nb;
-    for (uint64_t base = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) * kUnitsPerThread; base < n;
-         base += static_cast<uint64_t>(gridDim.x) * blockDim.x * kUnitsPerThread) {
-        uint64_t lo = 0, hi = nb;  // first bucket whose first unit is after `base`
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+        uint64_t lo = 0, hi = nb;  // first bucket whose first unit is after u
         while (lo < hi) {
             const uint64_t mid = (lo + hi) >> 1;
-            if (ustart[g0 + mid] <= base) lo = mid + 1;
+            if (ustart[g0 + mid] <= u) lo = mid + 1;
             else hi = mid;
         }
-        uint64_t g = g0 + lo - 1, have = ~0ull;
-        uint32_t c = 0, u0 = 0, lc = 0, ng = 1, q0 = 0;
-        uint64_t s = 0, e0 = 0, e1 = 0;
-        const uint64_t last = base + kUnitsPerThread < n ? base + kUnitsPerThread : n;
-        for (uint64_t u = base; u < last; u++) {
-            while (g + 1 < g_end && ustart[g + 1] <= u) g++;
-            if (g != have) {
-                have = g;
-                c = cnt[g];
-                u0 = ustart[g];
-                q0 = qstart[g];
-                s = slice_of_entry(off[g], n_sites, inv_n);
-                e0 = off[g] - s * n_sites;  // list positions
-                e1 = off[g + 1] - s * n_sites;
-                lc = __ffs(static_cast<uint32_t>(chunk_of(e1 - e0, cc))) - 1;  // unit sizes are powers of 2
-                ng = (c + kGroup - 1) / kGroup;
-            }
-            const uint32_t r = static_cast<uint32_t>(u) - u0;
-            const uint32_t k = r / ng, j = r - k * ng;
-            const uint64_t blk = (e0 >> lc) + k;
-            const uint64_t cb = (blk << lc) > e0 ? (blk << lc) : e0;
-            const uint64_t ce = ((blk + 1) << lc) < e1 ? ((blk + 1) << lc) : e1;
-            UnitDesc d;
-            d.p0 = static_cast<uint32_t>(cb);
-            d.qbeg = q0 + j * kGroup;
-            d.len = static_cast<uint16_t>(ce - cb);
-            d.qn = static_cast<uint8_t>(c - j * kGroup < kGroup ? c - j * kGroup : kGroup);
-            d.s = static_cast<uint8_t>(s);
-            d.pad = 0;
-            units[u] = d;
-        }
+        const uint64_t g = g0 + lo - 1;
+        const uint32_t c = cnt[g], r = u - ustart[g];
+        const uint64_t s = slice_of_entry(off[g], n_sites, inv_n);
+        const uint64_t e0 = off[g] - s * n_sites, e1 = off[g + 1] - s * n_sites;  // list positions
+        const uint32_t lc = __ffs(static_cast<uint32_t>(chunk_of(e1 - e0, cc))) - 1;  // unit sizes are powers of 2
+        const uint32_t ng = (c + kGroup - 1) / kGroup;
+        const uint32_t k = r / ng, j = r - k * ng;
+        const uint64_t blk = (e0 >> lc) + k;
+        const uint64_t cb = (blk << lc) > e0 ? (blk << lc) : e0;
+        const uint64_t ce = ((blk + 1) << lc) < e1 ? ((blk + 1) << lc) : e1;
+        UnitDesc d;
+        d.p0 = static_cast<uint32_t>(cb);
+        d.qbeg = qstart[g] + j * kGroup;
+        d.len = static_cast<uint16_t>(ce - cb);
+        d.qn = static_cast<uint8_t>(c - j * kGroup < kGroup ? c - j * kGroup : kGroup);
+        d.s = static_cast<uint8_t>(s);
+        d.pad = 0;
+        units[u] = d;
     }
 }
 
