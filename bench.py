@@ -341,6 +341,7 @@ def run_ours(args):
         "clocks": clocks.summary(),
         "probes_per_s": value * len(__import__("cracklingplusplus_gpu_b200").slice_masks(WORKLOAD["slice_config"])),
         "owned_hits_per_step": int(ix.last_stats().hits),
+        "dropped_hits_per_step": int(ix.last_stats().dropped_hits),
         "tuning": tuning,
         "generation_s": gen_s,
     }
@@ -609,7 +610,7 @@ def bench_capacity(args, pkg):
         "config": dict(CAPACITY, n_sites=n_sites, n_queries=nq, entry_bytes=info.entry_bytes,
                        resident_gb=info.device_bytes / 1e9, generation_s=gen_s),
         "stats": {"scan_ms": st.scan_ms, "scan_bytes": st.scan_bytes, "hits": st.hits, "candidates": st.candidates,
-                  "probes": st.probes, "launches": st.launches},
+                  "probes": st.probes, "launches": st.launches, "dropped_hits": st.dropped_hits},
         "tuning": tuning, "parity_sample": parity, "clocks": clocks.summary(),
     }
 

@@ -56,8 +56,9 @@ struct UnitDesc {   // 16 bytes
 struct Counters {
     // per wave (cleared at the start of every wave: the fields before `overflow`)
     uint64_t bucket_total;  // hi: units, lo: probes into non-empty buckets
+    unsigned long long cand_reserved;  // candidate slots reserved by the scan (may exceed capacity)
     uint32_t n_units;       // min(units, capacity)
-    uint32_t n_cand;        // hit slots reserved by the scan (may exceed capacity -> overflow)
+    uint32_t n_cand;        // min(cand_reserved, capacity): the slots the later kernels read
     uint32_t hit_total;     // owned hits: sum of per-guide hits (scan total)
     uint32_t n_big;         // exiting guides with more than kWarpSort hits (block scorer)
     uint32_t n_exit;        // exiting guides with at most kWarpSort hits (warp scorer)
@@ -73,6 +74,7 @@ struct Counters {
     uint64_t entries;       // entries compared by the scan (per guide group)
     uint64_t rbytes;        // bit-sliced bytes the scan copies
     uint64_t class_probes[3];  // probes into buckets of < 64, 64..4095, >= 4096 entries
+    uint64_t dropped;       // grouped hits whose site is farther than kMaxDist (counted for nothing)
 };
 constexpr size_t kWaveCounterBytes = offsetof(Counters, overflow);
 
@@ -117,7 +119,10 @@ __device__ __forceinline__ uint64_t chunk_of(uint64_t bucket_size, const ChunkCl
 constexpr int kMaxStages = 4;
 constexpr int kStageQr = kGroup + 2;     // (guide, residual) pairs per stage + alignment slack
 constexpr uint32_t kCandSlab = 256;
+// candidate slots of one wave are addressed with 32 bits: the capacity stays below this
+constexpr size_t kMaxCandSlots = 0xFFFFFFFFull - (1ull << 20);
 constexpr uint32_t kDeadCand = 0xFFFFFFFFu;  // guide field of an unused or rejected candidate slot
+constexpr uint32_t kNoSite = 0xFFFFFFFFu;  // grouped-hit id of a record that counts for nothing
 constexpr int kGuideBits = 26;               // candidate records pack guide | slice << 26
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 1.965 GHz
 
@@ -336,42 +341,73 @@ __device__ __forceinline__ uint64_t slice_of_entry(uint64_t e, uint64_t n, doubl
     return s;
 }
 
-// Unit descriptors, one thread per unit. The unit's bucket is the last bucket of the wave whose
-// first unit is at or before it (binary search of the units' exclusive prefix; empty buckets share
-// their successor's prefix, so the search lands on the bucket that owns the unit). A bucket's
+// Unit descriptors, kUnitsPerThread consecutive units per thread. The first unit's bucket is the
+// last bucket of the wave whose first unit is at or before it (binary search of the units'
+// exclusive prefix; empty buckets share their successor's prefix, so the search lands on the
+// bucket that owns the unit). The following units stay in that bucket or gallop forward to theirs
+// (a walk one bucket at a time would crawl over the empty buckets of sparse waves). A bucket's
 // units run over the chunk-aligned blocks of its list range, and within a block over its groups
-// of up to kGroup guides. (Walking forward from one search to the next units instead is no faster
-// on dense waves and crawls over the empty buckets of sparse ones.)
+// of up to kGroup guides.
+constexpr uint32_t kUnitsPerThread = 8;
 __global__ void k_expand_units(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off,
                                const uint32_t* __restrict__ qstart, const uint32_t* __restrict__ ustart, uint64_t g0,
                                uint64_t nb, uint64_t n_sites, double inv_n, ChunkClasses cc,
                                const Counters* __restrict__ ctr, UnitDesc* __restrict__ units) {
     const uint32_t n = ctr->n_units;  // at most the buffer's capacity
-    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
-        uint64_t lo = 0, hi = nb;  // first bucket whose first unit is after u
+    const uint64_t g_end = g0 + nb;
+    for (uint64_t base = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) * kUnitsPerThread; base < n;
+         base += static_cast<uint64_t>(gridDim.x) * blockDim.x * kUnitsPerThread) {
+        uint64_t lo = 0, hi = nb;  // first bucket whose first unit is after `base`
         while (lo < hi) {
             const uint64_t mid = (lo + hi) >> 1;
-            if (ustart[g0 + mid] <= u) lo = mid + 1;
+            if (ustart[g0 + mid] <= base) lo = mid + 1;
             else hi = mid;
         }
-        const uint64_t g = g0 + lo - 1;
-        const uint32_t c = cnt[g], r = u - ustart[g];
-        const uint64_t s = slice_of_entry(off[g], n_sites, inv_n);
-        const uint64_t e0 = off[g] - s * n_sites, e1 = off[g + 1] - s * n_sites;  // list positions
-        const uint32_t lc = __ffs(static_cast<uint32_t>(chunk_of(e1 - e0, cc))) - 1;  // unit sizes are powers of 2
-        const uint32_t ng = (c + kGroup - 1) / kGroup;
-        const uint32_t k = r / ng, j = r - k * ng;
-        const uint64_t blk = (e0 >> lc) + k;
-        const uint64_t cb = (blk << lc) > e0 ? (blk << lc) : e0;
-        const uint64_t ce = ((blk + 1) << lc) < e1 ? ((blk + 1) << lc) : e1;
-        UnitDesc d;
-        d.p0 = static_cast<uint32_t>(cb);
-        d.qbeg = qstart[g] + j * kGroup;
-        d.len = static_cast<uint16_t>(ce - cb);
-        d.qn = static_cast<uint8_t>(c - j * kGroup < kGroup ? c - j * kGroup : kGroup);
-        d.s = static_cast<uint8_t>(s);
-        d.pad = 0;
-        units[u] = d;
+        uint64_t g = g0 + lo - 1, have = ~0ull;
+        uint32_t c = 0, u0 = 0, lc = 0, ng = 1, q0 = 0;
+        uint64_t s = 0, e0 = 0, e1 = 0;
+        const uint64_t last = base + kUnitsPerThread < n ? base + kUnitsPerThread : n;
+        for (uint64_t u = base; u < last; u++) {
+            if (g + 1 < g_end && ustart[g + 1] <= u) {  // u is in a later bucket: gallop, then bisect
+                uint64_t a = g + 1, b = a + 1, step = 1;  // ustart[a] <= u
+                while (b < g_end && ustart[b] <= u) {
+                    a = b;
+                    step <<= 1;
+                    b = a + step;
+                }
+                if (b > g_end) b = g_end;  // b == g_end or ustart[b] > u
+                while (b - a > 1) {
+                    const uint64_t mid = (a + b) >> 1;
+                    if (ustart[mid] <= u) a = mid;
+                    else b = mid;
+                }
+                g = a;
+            }
+            if (g != have) {
+                have = g;
+                c = cnt[g];
+                u0 = ustart[g];
+                q0 = qstart[g];
+                s = slice_of_entry(off[g], n_sites, inv_n);
+                e0 = off[g] - s * n_sites;  // list positions
+                e1 = off[g + 1] - s * n_sites;
+                lc = __ffs(static_cast<uint32_t>(chunk_of(e1 - e0, cc))) - 1;  // unit sizes are powers of 2
+                ng = (c + kGroup - 1) / kGroup;
+            }
+            const uint32_t r = static_cast<uint32_t>(u) - u0;
+            const uint32_t k = r / ng, j = r - k * ng;
+            const uint64_t blk = (e0 >> lc) + k;
+            const uint64_t cb = (blk << lc) > e0 ? (blk << lc) : e0;
+            const uint64_t ce = ((blk + 1) << lc) < e1 ? ((blk + 1) << lc) : e1;
+            UnitDesc d;
+            d.p0 = static_cast<uint32_t>(cb);
+            d.qbeg = q0 + j * kGroup;
+            d.len = static_cast<uint16_t>(ce - cb);
+            d.qn = static_cast<uint8_t>(c - j * kGroup < kGroup ? c - j * kGroup : kGroup);
+            d.s = static_cast<uint8_t>(s);
+            d.pad = 0;
+            units[u] = d;
+        }
     }
 }
 
@@ -533,11 +569,17 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
                 // retire the rest of the slab, reserve a new one
                 for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
                     if (i < a.cand_cap) a.cands[i] = make_uint4(kDeadCand, 0, 0, 0);
-                uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(&a.counters->n_cand, kCandSlab);
+                // 64-bit reservations: a wave may ask for more than 2^32 slots (the host then splits
+                // the guides); a slab past the capacity is never written
+                uint32_t base = 0, full = 0;
+                if (lane == 0) {
+                    const unsigned long long b = atomicAdd(&a.counters->cand_reserved, static_cast<unsigned long long>(kCandSlab));
+                    full = b + kCandSlab > a.cand_cap;
+                    base = full ? a.cand_cap : static_cast<uint32_t>(b);
+                }
                 cx.cpos = __shfl_sync(0xffffffffu, base, 0);
                 cx.cend = cx.cpos + kCandSlab;
-                cx.full = cx.cend > a.cand_cap;
+                cx.full = __shfl_sync(0xffffffffu, full, 0) != 0;
             }
             if (cbits) {
                 const int e = __ffs(cbits) - 1;
@@ -697,9 +739,11 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
 }
 
 __global__ void k_cands_finalize(Counters* c, uint32_t cand_cap) {
-    if (c->n_cand > cand_cap) atomicOr(&c->overflow, 2u);
-    if (c->n_cand > c->max_cand) c->max_cand = c->n_cand;
-    c->cands += c->n_cand;
+    const unsigned long long r = c->cand_reserved;
+    if (r > cand_cap) atomicOr(&c->overflow, 2u);
+    if (r > c->max_cand) c->max_cand = r;
+    c->cands += r;
+    c->n_cand = static_cast<uint32_t>(r < cand_cap ? r : cand_cap);
 }
 
 // 5. the ownership rule on the candidates: a site reached in slice s is counted only if no
@@ -783,7 +827,7 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
     c.occ = occ;
     c.mit = 0.0;
     c.cfd = 0.0;
-    if (P.calc_mit && dist > 0) {
+    if (P.calc_mit && dist > 0 && dist <= kMaxDist) {  // the table holds 1..4 mismatches
         uint32_t rank = 0, i = 0, mm = m20;
         while (mm) {
             const int p = __ffs(mm) - 1;
@@ -838,7 +882,17 @@ __global__ void k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint
         uint32_t id, occ;
         uint64_t sig;
         load_site(ix, sl, r.y, gq, g[sl], id, occ, sig);
-        const Contribution ct = contribution(T, both, gq, sig, occ);
+        // A scored site is within kMaxDist of the guide by construction (its slice positions
+        // match and the scan bounds the rest). Should a record ever say otherwise, it counts for
+        // nothing: no occurrences, no scores, no distinct site.
+        Contribution ct{0.0, 0.0, 0u};
+        if (__popcll(fold64(gq ^ sig)) <= kMaxDist) {
+            ct = contribution(T, both, gq, sig, occ);
+        } else {
+            occ = 0;
+            id = kNoSite;
+            atomicAdd(reinterpret_cast<unsigned long long*>(&c->dropped), 1ull);
+        }
         // the decrement leaves qhits all zero for the next call
         const uint32_t slot = qhoff[q] + atomicSub(&qhits[q], 1u) - 1u;
         seg[slot] = HitRec{make_uint4(r.y, sl, id, occ), ct.mit, ct.cfd};
@@ -1031,7 +1085,7 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         if (P.want_distinct)
             for (uint32_t j = lane; j < L; j += 32) {
                 const uint32_t id = seg[j].r.z;
-                atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
         if (lane == 0) {
             if (a.last_wave) {
@@ -1137,7 +1191,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             if (P.want_distinct)
                 for (uint32_t j = lane; j < L; j += 32) {
                     const uint32_t id = seg[j].r.z;
-                    atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                    if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
                 }
             if (lane == 0) finalise(P, fx_double(cm), fx_double(cc), cn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
             __syncwarp();
@@ -1147,7 +1201,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
         if (P.want_distinct)  // the sites of the slices before the exit slice
             for (uint32_t j = lane; j < b0; j += 32) {
                 const uint32_t id = seg[W.idx[j]].r.z;
-                atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
         rm = bm;
         rc = bc;
@@ -1191,7 +1245,8 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
                 const bool ex = t < ns && exit_test(P, fx_double(im), fx_double(ic));
                 const unsigned em = __ballot_sync(0xffffffffu, ex);
                 const int last = em ? __ffs(em) - 1 : (ns - c0 >= 32 ? 31 : static_cast<int>(ns - c0 - 1));
-                if (P.want_distinct && t < ns && lane <= last) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                if (P.want_distinct && t < ns && lane <= last && id != kNoSite)
+                    atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
                 rm = Fx{__shfl_sync(0xffffffffu, im.hi, last), __shfl_sync(0xffffffffu, im.lo, last)};
                 rc = Fx{__shfl_sync(0xffffffffu, ic.hi, last), __shfl_sync(0xffffffffu, ic.lo, last)};
                 rn = __shfl_sync(0xffffffffu, in, last);
@@ -1297,7 +1352,7 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             const uint32_t in_chunk = L - c0 < blockDim.x ? L - c0 : blockDim.x;
             const int last = first != 0x7fffffff ? first : static_cast<int>(in_chunk) - 1;
             if (P.want_distinct && t < L && static_cast<int>(threadIdx.x) <= last)
-                atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             __syncthreads();
             if (static_cast<int>(threadIdx.x) == last) {
                 s_wm[0] = im;
@@ -1417,7 +1472,9 @@ void apply_tuning(issl_index* ix, Workspace& ws) {
 }
 
 // A failed allocation leaves some buffers released: forget every capacity so that the next call
-// reallocates what is missing (and re-zeroes the counters that must start at zero).
+// reallocates what is missing (and re-zeroes the counters that must start at zero). (Freeing the
+// large buffers outright here made calls at the edge of device memory reallocate tens of GB on
+// every call: 956 instead of 634 ms on the 500M-site capacity workload.)
 template <class F>
 void with_alloc_guard(Workspace& ws, F&& f) {
     try {
@@ -1554,8 +1611,9 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
     // device, which stalls concurrent work); grown on demand after an overflow
     size_t want_cands = static_cast<size_t>(static_cast<double>(n) * ws.cand_density * 1.1) + 65536 +
                         static_cast<size_t>(ws.scan_blocks) * kScanWarps * kCandSlab;
+    want_cands = std::min(want_cands, kMaxCandSlots);
     if (ws.cand_cap < want_cands) {
-        want_cands = std::max<size_t>(want_cands, ws.cand_cap + ws.cand_cap / 2);
+        want_cands = std::min(std::max<size_t>(want_cands, ws.cand_cap + ws.cand_cap / 2), kMaxCandSlots);
         ws.cands.reserve(want_cands);
         ws.seg.reserve(want_cands);
         ws.cand_cap = want_cands;
@@ -1802,8 +1860,10 @@ bool check_and_grow(Workspace& ws, cudaStream_t st) {
         }
         if (c.max_cand > ws.cand_cap || (c.overflow & 2u)) {
             const size_t cap = static_cast<size_t>(c.max_cand) + c.max_cand / 4 + 65536;
-            ISSL_REQUIRE(cap < 0xFFFFFFFFull, ISSL_ERR_UNSUPPORTED,
-                         "more than 2^32 candidate sites in one slice wave; split the guides");
+            // beyond 32-bit slot numbers: report it like a failed allocation, so that the caller
+            // splits the guides into chunks (run_scoring / run_batch_chunked)
+            ISSL_REQUIRE(cap <= kMaxCandSlots, ISSL_ERR_NOMEM,
+                         "more than 2^32 candidate sites in one slice wave for these guides");
             ws.cands.reserve(cap);
             ws.seg.reserve(cap);
             ws.cand_cap = cap;
@@ -1832,6 +1892,7 @@ void fill_stats(const Workspace& ws, float scan_ms, float total_ms, uint64_t lau
     for (int i = 0; i < 3; i++) s.class_probes[i] = ws.last.class_probes[i];
     s.candidates = ws.last.cands;
     s.staged_bytes = ws.staged;
+    s.dropped_hits = ws.last.dropped;
 }
 
 issl_score_stats run_stats(issl_index* ix, Workspace& ws) {
@@ -1862,6 +1923,7 @@ void add_stats(issl_score_stats& a, const issl_score_stats& b) {
     for (int i = 0; i < 3; i++) a.class_probes[i] += b.class_probes[i];
     a.candidates += b.candidates;
     a.staged_bytes += b.staged_bytes;
+    a.dropped_hits += b.dropped_hits;
 }
 
 // One pipeline run over n guides, growing the workspace and rerunning on overflow.

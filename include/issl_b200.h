@@ -172,6 +172,8 @@ typedef struct {
     uint64_t class_probes[3];   /* probes into buckets of < 64, 64..4095 and >= 4096 entries */
     uint64_t candidates;        /* candidate slots the scan wrote, before the ownership rule */
     uint64_t staged_bytes;      /* host-list index: list bytes copied from host memory */
+    uint64_t dropped_hits;      /* candidate sites found farther than 4 mismatches from their guide
+                                   (none by construction; counted for nothing if ever seen) */
 } issl_score_stats;
 
 /* Frees the device memory of the index's own scoring workspace (the buffers the plain
