@@ -341,7 +341,8 @@ __device__ __forceinline__ uint64_t slice_of_entry(uint64_t e, uint64_t n, doubl
     return s;
 }
 
-// Unit descriptors, kUnitsPerThread consecutive units per thread. The first unit's bucket is the
+// Unit descriptors, up to kUnitsPerThread consecutive units per thread (one when the units are too
+// few to give every thread of the grid several). The first unit's bucket is the
 // last bucket of the wave whose first unit is at or before it (binary search of the units'
 // exclusive prefix; empty buckets share their successor's prefix, so the search lands on the
 // bucket that owns the unit). The following units stay in that bucket or gallop forward to theirs
@@ -355,8 +356,10 @@ __global__ void k_expand_units(const uint32_t* __restrict__ cnt, const uint64_t*
                                const Counters* __restrict__ ctr, UnitDesc* __restrict__ units) {
     const uint32_t n = ctr->n_units;  // at most the buffer's capacity
     const uint64_t g_end = g0 + nb;
-    for (uint64_t base = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) * kUnitsPerThread; base < n;
-         base += static_cast<uint64_t>(gridDim.x) * blockDim.x * kUnitsPerThread) {
+    const uint64_t threads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t upt = std::min<uint64_t>(kUnitsPerThread, std::max<uint64_t>(1, (n + threads - 1) / threads));
+    for (uint64_t base = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) * upt; base < n;
+         base += threads * upt) {
         uint64_t lo = 0, hi = nb;  // first bucket whose first unit is after `base`
         while (lo < hi) {
             const uint64_t mid = (lo + hi) >> 1;
@@ -366,7 +369,7 @@ __global__ void k_expand_units(const uint32_t* __restrict__ cnt, const uint64_t*
         uint64_t g = g0 + lo - 1, have = ~0ull;
         uint32_t c = 0, u0 = 0, lc = 0, ng = 1, q0 = 0;
         uint64_t s = 0, e0 = 0, e1 = 0;
-        const uint64_t last = base + kUnitsPerThread < n ? base + kUnitsPerThread : n;
+        const uint64_t last = base + upt < n ? base + upt : n;
         for (uint64_t u = base; u < last; u++) {
             if (g + 1 < g_end && ustart[g + 1] <= u) {  // u is in a later bucket: gallop, then bisect
                 uint64_t a = g + 1, b = a + 1, step = 1;  // ustart[a] <= u
@@ -815,6 +818,7 @@ __device__ __forceinline__ uint64_t order_key(const uint4& r) {
 struct Contribution {
     double mit, cfd;
     uint32_t occ;
+    int dist;  // mismatches between the guide and the site
 };
 
 // MIT (ISSLScoringModule.cpp:294-298) and CFD (:301-363) contributions of one site.
@@ -827,6 +831,7 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
     c.occ = occ;
     c.mit = 0.0;
     c.cfd = 0.0;
+    c.dist = dist;
     if (P.calc_mit && dist > 0 && dist <= kMaxDist) {  // the table holds 1..4 mismatches
         uint32_t rank = 0, i = 0, mm = m20;
         while (mm) {
@@ -860,9 +865,11 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
 // with 4-byte entries the signature is a second read. The hit's MIT and CFD contributions are
 // computed here, where the random reads leave the arithmetic units idle, and written into the
 // guide's segment so that the scorers read only contiguous data.
-__global__ void k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint32_t* __restrict__ qhits,
-                              const uint32_t* __restrict__ qhoff, IndexView ix, const uint64_t* __restrict__ qsig,
-                              const Tables* __restrict__ tables, HitRec* __restrict__ seg) {
+// (32 registers: eight blocks of 256 threads per SM keep the most random reads in flight)
+__global__ void __launch_bounds__(256, 8)
+    k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint32_t* __restrict__ qhits,
+                  const uint32_t* __restrict__ qhoff, IndexView ix, const uint64_t* __restrict__ qsig,
+                  const Tables* __restrict__ tables, HitRec* __restrict__ seg) {
     __shared__ SliceGeom g[kMaxSlices];
     for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
     __syncthreads();
@@ -885,10 +892,9 @@ __global__ void k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint
         // A scored site is within kMaxDist of the guide by construction (its slice positions
         // match and the scan bounds the rest). Should a record ever say otherwise, it counts for
         // nothing: no occurrences, no scores, no distinct site.
-        Contribution ct{0.0, 0.0, 0u};
-        if (__popcll(fold64(gq ^ sig)) <= kMaxDist) {
-            ct = contribution(T, both, gq, sig, occ);
-        } else {
+        Contribution ct = contribution(T, both, gq, sig, occ);
+        if (ct.dist > kMaxDist) {
+            ct.mit = ct.cfd = 0.0;
             occ = 0;
             id = kNoSite;
             atomicAdd(reinterpret_cast<unsigned long long*>(&c->dropped), 1ull);
