@@ -13,7 +13,8 @@ OT_METHODS = {"mit": 0, "cfd": 1, "mitAndCfd": 2, "mitOrCfd": 3, "avgMitCfd": 4}
 CLI_METHODS = {"mit": 0, "cfd": 1, "and": 2, "or": 3, "avg": 4}
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "I/O error", -3: "format error", -4: "out of memory",
-          -5: "CUDA error", -6: "timeout", -7: "unsupported", -8: "busy"}
+          -5: "CUDA error", -6: "timeout", -7: "unsupported", -8: "busy",
+          -9: "internal consistency check failed"}
 
 
 class IsslError(RuntimeError):
@@ -36,7 +37,7 @@ class ScoreStats(C.Structure):
                 ("buckets_scanned", C.c_uint64), ("entries_scanned", C.c_uint64), ("units", C.c_uint64),
                 ("hits", C.c_uint64), ("scan_bytes", C.c_uint64), ("launches", C.c_uint64),
                 ("class_probes", C.c_uint64 * 3), ("candidates", C.c_uint64), ("staged_bytes", C.c_uint64),
-                ("dropped_hits", C.c_uint64)]
+                ("dropped_hits", C.c_uint64), ("replayed", C.c_uint64)]
 
 
 class Tuning(C.Structure):
@@ -139,6 +140,7 @@ SIGNATURES = [
                                   C.c_char_p, C.c_size_t, P(C.c_uint8), P(C.c_int8), C.c_char_p, f64p, f64p,
                                   C.c_char_p]),
     ("issl_module_release_all", C.c_int, []),
+    ("issl_module_open", C.c_int, [C.c_char_p, C.c_int, C.c_int, P(vp)]),
 ]
 
 

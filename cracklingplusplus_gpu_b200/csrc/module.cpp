@@ -1,154 +1,110 @@
-// ISSLScoringModule on the B200 library: lib/ISSLScoringModule.cpp:13-513 with the scoring loop
-// replaced by issl_score() and the per-call file read replaced by a resident index.
-#include "issl_b200_module.hpp"
-
-#include <cstdio>
+// The C entry points behind the header-only ISSLScoringModule (include/issl_b200_module.hpp):
+// lib/ISSLScoringModule.cpp:13-513 with the scoring loop replaced by issl_score() and the per-call
+// file read replaced by a resident index. Only C types cross this boundary, so the library
+// exports no C++ symbol tied to the layout of cracklingConfig or guideResults.
 #include <cstdlib>
 #include <cstring>
-#include <iostream>
 #include <map>
 #include <mutex>
-#include <stdexcept>
+#include <string>
+#include <vector>
 
-namespace issl {
-void set_last_error(const std::string& msg);
+#include "issl_internal.cuh"
+
+extern "C" {
+int issl_module_open(const char* index_path, int device, int memory_mapped, issl_index** out);
+int issl_module_run(const char* index_path, int method, double threshold, int optimisation, int consensus_n,
+                    int flags, size_t n, const char* seqs, size_t stride, const uint8_t* is_unique,
+                    const int8_t* consensus_count, const char* passed_bowtie2, double* mit_out, double* cfd_out,
+                    char* code_out);
+int issl_module_release_all(void);
 }
 
 namespace {
 
-// keeps the library status next to the reference's exception type
-struct ModuleError : std::runtime_error {
-    int code;
-    ModuleError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
+constexpr int kModuleEnabled = 1;       // ISSL_MODULE_ENABLED
+constexpr int kModuleMemoryMapped = 2;  // ISSL_MODULE_MEMORY_MAPPED
+// optimisationLevel, include/util.hpp:21
+constexpr int kUltralow = 0, kMedium = 2, kHigh = 3;
 
 std::mutex g_cache_mu;
 std::map<std::string, issl_index*> g_cache;  // indexes kept open, keyed by (path, device, mapped)
 
-// The index of a path, opened on first use and kept for the process. memoryMapped selects the
-// host-list index (ISSLScoringModuleMMF's role); ISSL_WINDOW_SLICES sets its window (default 4).
-issl_index* resident_index(const std::string& path, int device, bool mapped) {
-    std::lock_guard<std::mutex> lock(g_cache_mu);
-    const std::string key = path + "#" + std::to_string(device) + (mapped ? "#mapped" : "");
-    auto it = g_cache.find(key);
-    if (it != g_cache.end()) return it->second;
-    issl_index* ix = nullptr;
-    const char* w = std::getenv("ISSL_WINDOW_SLICES");
-    const int rc = mapped ? issl_open_mapped(path.c_str(), device, w ? static_cast<uint32_t>(std::atoi(w)) : 4u, &ix)
-                          : issl_open(path.c_str(), device, &ix);
-    if (rc != ISSL_OK) throw ModuleError(rc, issl_last_error());
-    g_cache[key] = ix;
-    return ix;
-}
-
-}  // namespace
-
-ISSLScoringModule::ISSLScoringModule(const cracklingConfig& cfg) {
-    // specificityModule::specificityModule, lib/specificityModule.cpp:3-8
-    toolIsSelected = cfg.offTarget.enabled;
-    optimsationLevel = cfg.general.optimisation;
-    consensusN = cfg.consensus.n;
-    config = cfg.offTarget;
-    ISSLIndex = cfg.input.offtargetSites;
-    const char* dev = std::getenv("ISSL_DEVICE");
-    device = dev ? std::atoi(dev) : 0;
-    switch (config.method) {  // lib/ISSLScoringModule.cpp:24-49
-        case otScoreMethod::mitAndCfd:
-        case otScoreMethod::mitOrCfd:
-        case otScoreMethod::avgMitCfd:
-        case otScoreMethod::mit:
-        case otScoreMethod::cfd:
-            break;
-        default:
-            throw std::runtime_error("Scoring method is not valid.");
-    }
-}
-
-bool ISSLScoringModule::processGuide(const guideResults& guide) const {
-    // lib/ISSLScoringModule.cpp:488-513
-    if (optimsationLevel == optimisationLevel::ultralow) return true;
-    if (!guide.isUnique) return false;
-    if (optimsationLevel == optimisationLevel::medium || optimsationLevel == optimisationLevel::high) {
-        if (guide.consensusCount < consensusN) return false;
-        if (guide.passedBowtie2 == ISSL_CODE_REJECTED) return false;
+// processGuide, lib/ISSLScoringModule.cpp:488-513
+bool process_guide(int optimisation, int consensus_n, bool is_unique, int consensus_count, char passed_bowtie2) {
+    if (optimisation == kUltralow) return true;
+    if (!is_unique) return false;
+    if (optimisation == kMedium || optimisation == kHigh) {
+        if (consensus_count < consensus_n) return false;
+        if (passed_bowtie2 == ISSL_CODE_REJECTED) return false;
     }
     return true;
 }
 
-void ISSLScoringModule::run(std::vector<guideResults>& candidateGuides) {
-    if (!toolIsSelected) {
-        std::cout << "Off-target scoring has been configured not to run. Skipping Off-target scoring" << std::endl;
-        return;
-    }
-    issl_index* ix = resident_index(ISSLIndex.string(), device, config.memoryMapped);
-    std::vector<size_t> picked;
-    picked.reserve(candidateGuides.size());
-    for (size_t i = 0; i < candidateGuides.size(); i++)
-        if (processGuide(candidateGuides[i])) picked.push_back(i);
-    const size_t n = picked.size();
-    std::vector<char> seqs(n * 20, 0);
-    for (size_t k = 0; k < n; k++) {
-        const std::string& s = candidateGuides[picked[k]].seq;
-        std::memcpy(seqs.data() + 20 * k, s.data(), s.size() < 20 ? s.size() : 20);
-    }
-    std::vector<double> mit(n), cfd(n);
-    std::vector<char> code(n);
-    if (n) {
-        const int rc = issl_score(ix, seqs.data(), 20, n, static_cast<int>(config.method), config.scoreThreshold, 4,
-                                  mit.data(), cfd.data(), code.data(), nullptr, nullptr);
-        if (rc != ISSL_OK) throw ModuleError(rc, issl_last_error());
-    }
-    size_t failed = 0;
-    for (size_t k = 0; k < n; k++) {
-        guideResults& g = candidateGuides[picked[k]];
-        g.mitOfftargetscore = mit[k];
-        g.cfdOfftargetscore = cfd[k];
-        g.passedOffTargetScore = code[k];
-        failed += code[k] == ISSL_CODE_REJECTED;
-    }
-    std::cout << "\t" << failed << " of " << n << " failed here." << std::endl;
+}  // namespace
+
+extern "C" int issl_module_open(const char* index_path, int device, int memory_mapped, issl_index** out) {
+    return issl::guarded([&] {
+        ISSL_REQUIRE(index_path && out, ISSL_ERR_ARG, "issl_module_open: null argument");
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        const std::string key = std::string(index_path) + "#" + std::to_string(device) + (memory_mapped ? "#mapped" : "");
+        auto it = g_cache.find(key);
+        if (it != g_cache.end()) {
+            *out = it->second;
+            return;
+        }
+        issl_index* ix = nullptr;
+        const char* w = std::getenv("ISSL_WINDOW_SLICES");
+        const int rc = memory_mapped
+                           ? issl_open_mapped(index_path, device, w ? static_cast<uint32_t>(std::atoi(w)) : 4u, &ix)
+                           : issl_open(index_path, device, &ix);
+        if (rc != ISSL_OK) throw issl::Error(rc, issl_last_error());
+        g_cache[key] = ix;
+        *out = ix;
+    });
 }
 
 extern "C" int issl_module_run(const char* index_path, int method, double threshold, int optimisation,
                                int consensus_n, int flags, size_t n, const char* seqs, size_t stride,
                                const uint8_t* is_unique, const int8_t* consensus_count, const char* passed_bowtie2,
                                double* mit_out, double* cfd_out, char* code_out) {
-    try {
-        if (!index_path || (n && (!seqs || !mit_out || !cfd_out || !code_out))) return ISSL_ERR_ARG;
-        cracklingConfig cfg;
-        cfg.input.offtargetSites = index_path;
-        cfg.offTarget.method = static_cast<otScoreMethod>(method);
-        cfg.offTarget.scoreThreshold = threshold;
-        cfg.offTarget.enabled = (flags & ISSL_MODULE_ENABLED) != 0;
-        cfg.offTarget.memoryMapped = (flags & ISSL_MODULE_MEMORY_MAPPED) != 0;
-        cfg.general.optimisation = static_cast<optimisationLevel>(optimisation);
-        cfg.consensus.n = static_cast<uint8_t>(consensus_n);
-        std::vector<guideResults> guides(n);
-        for (size_t i = 0; i < n; i++) {
-            const char* s = seqs + i * stride;
-            guides[i].seq.assign(s, strnlen(s, stride));
-            guides[i].isUnique = is_unique ? is_unique[i] != 0 : true;
-            guides[i].consensusCount = consensus_count ? consensus_count[i] : 0;
-            guides[i].passedBowtie2 = passed_bowtie2 ? passed_bowtie2[i] : '?';
-            // outputs are in/out: guides the filter skips keep what the caller passed in
-            guides[i].mitOfftargetscore = mit_out[i];
-            guides[i].cfdOfftargetscore = cfd_out[i];
-            guides[i].passedOffTargetScore = code_out[i];
+    return issl::guarded([&] {
+        ISSL_REQUIRE(index_path && (n == 0 || (seqs && mit_out && cfd_out && code_out)), ISSL_ERR_ARG,
+                     "issl_module_run: null argument");
+        // lib/ISSLScoringModule.cpp:24-49
+        ISSL_REQUIRE(method >= ISSL_METHOD_MIT && method <= ISSL_METHOD_AVG_MIT_CFD, ISSL_ERR_ARG,
+                     "Scoring method is not valid.");
+        if (!(flags & kModuleEnabled)) return;  // the tool is not selected: nothing is touched
+        std::vector<size_t> picked;
+        picked.reserve(n);
+        for (size_t i = 0; i < n; i++)
+            if (process_guide(optimisation, consensus_n, is_unique ? is_unique[i] != 0 : true,
+                              consensus_count ? consensus_count[i] : 0, passed_bowtie2 ? passed_bowtie2[i] : '?'))
+                picked.push_back(i);
+        const size_t k = picked.size();
+        if (!k) return;
+        const char* dev = std::getenv("ISSL_DEVICE");
+        issl_index* ix = nullptr;
+        const int rc = issl_module_open(index_path, dev ? std::atoi(dev) : 0, (flags & kModuleMemoryMapped) != 0, &ix);
+        if (rc != ISSL_OK) throw issl::Error(rc, issl_last_error());
+        // sequenceToSignature(seq, 20) reads the first 20 characters (:219, :469-476); a shorter
+        // sequence reads as if padded with A
+        std::vector<char> packed(k * issl::kSeqLen, 'A');
+        for (size_t j = 0; j < k; j++) {
+            const char* s = seqs + picked[j] * stride;
+            std::memcpy(packed.data() + j * issl::kSeqLen, s, strnlen(s, std::min<size_t>(stride, issl::kSeqLen)));
         }
-        ISSLScoringModule module(cfg);
-        module.run(guides);
-        for (size_t i = 0; i < n; i++) {
-            mit_out[i] = guides[i].mitOfftargetscore;
-            cfd_out[i] = guides[i].cfdOfftargetscore;
-            code_out[i] = guides[i].passedOffTargetScore;
+        std::vector<double> mit(k), cfd(k);
+        std::vector<char> code(k);
+        const int rs = issl_score(ix, packed.data(), issl::kSeqLen, k, method, threshold, issl::kMaxDist, mit.data(),
+                                  cfd.data(), code.data(), nullptr, nullptr);
+        if (rs != ISSL_OK) throw issl::Error(rs, issl_last_error());
+        for (size_t j = 0; j < k; j++) {
+            mit_out[picked[j]] = mit[j];
+            cfd_out[picked[j]] = cfd[j];
+            code_out[picked[j]] = code[j];
         }
-        return ISSL_OK;
-    } catch (const ModuleError& e) {
-        return e.code;
-    } catch (const std::exception& e) {
-        issl::set_last_error(e.what());
-        return ISSL_ERR_ARG;
-    }
+    });
 }
 
 extern "C" int issl_module_release_all(void) {

@@ -66,7 +66,7 @@ struct Counters {
     // per call
     uint32_t overflow;      // 1: units, 2: hits, 4: a bounded wait in the scan gave up
     uint32_t act_n[2];      // guides still scoring after a wave (active lists A and B)
-    uint32_t pad;
+    uint32_t n_replay;      // guides rescored by k_replay (decision within the reference's rounding)
     uint64_t max_units, max_cand;        // largest wave (to size the buffers)
     uint64_t probes, units, hits, cands; // summed over the waves
     uint64_t distinct;
@@ -191,6 +191,7 @@ struct issl::Workspace {
     DevBuf<uint4> cands;  // candidate slots
     DevBuf<HitRec> seg;   // owned hits grouped per guide
     DevBuf<uint32_t> qhits, qhoff, big, exitq;
+    DevBuf<uint32_t> replayq;  // guides whose decision k_replay settles
     DevBuf<uint32_t> bitmap;
     DevBuf<Counters> counters;
     DevBuf<uint64_t> scan64;
@@ -891,7 +892,8 @@ __global__ void __launch_bounds__(256, 8)
         load_site(ix, sl, r.y, gq, g[sl], id, occ, sig);
         // A scored site is within kMaxDist of the guide by construction (its slice positions
         // match and the scan bounds the rest). Should a record ever say otherwise, it counts for
-        // nothing: no occurrences, no scores, no distinct site.
+        // nothing here (no occurrences, no scores, no distinct site, and the MIT table is never
+        // indexed out of range) and the call fails with ISSL_ERR_INTERNAL.
         Contribution ct = contribution(T, both, gq, sig, occ);
         if (ct.dist > kMaxDist) {
             ct.mit = ct.cfd = 0.0;
@@ -916,23 +918,68 @@ __device__ __forceinline__ bool exit_test(const ScoreParams& P, double mit, doub
     }
 }
 
+// The accept rule on the sums where scoring stopped (:404-459).
+__device__ __forceinline__ bool rejects(const ScoreParams& P, double tot_mit, double tot_cfd) {
+    const double t = P.threshold;
+    const double m = 10000.0 / (100.0 + tot_mit), c = 10000.0 / (100.0 + tot_cfd);  // :407-448
+    switch (P.method) {
+        case ISSL_METHOD_MIT_AND_CFD: return m < t && c < t;
+        case ISSL_METHOD_MIT_OR_CFD: return m < t || c < t;
+        case ISSL_METHOD_AVG_MIT_CFD: return (m + c) / 2 < t;
+        case ISSL_METHOD_MIT: return m < t;
+        default: return c < t;
+    }
+}
+
 __device__ __forceinline__ void finalise(const ScoreParams& P, double tot_mit, double tot_cfd, uint64_t count,
                                          uint64_t q_index, double* out_mit, double* out_cfd, char* out_code,
                                          uint64_t* out_count) {
-    const double t = P.threshold;
-    double m = 10000.0 / (100.0 + tot_mit), c = 10000.0 / (100.0 + tot_cfd);  // :407-448
-    bool reject;
-    switch (P.method) {
-        case ISSL_METHOD_MIT_AND_CFD: reject = m < t && c < t; break;
-        case ISSL_METHOD_MIT_OR_CFD: reject = m < t || c < t; break;
-        case ISSL_METHOD_AVG_MIT_CFD: reject = (m + c) / 2 < t; break;
-        case ISSL_METHOD_MIT: reject = m < t; c = -1; break;
-        default: reject = c < t; m = -1; break;
-    }
+    const bool reject = rejects(P, tot_mit, tot_cfd);
+    const double m = P.method == ISSL_METHOD_CFD ? -1.0 : 10000.0 / (100.0 + tot_mit);
+    const double c = P.method == ISSL_METHOD_MIT ? -1.0 : 10000.0 / (100.0 + tot_cfd);
     if (out_mit) out_mit[q_index] = m;
     if (out_cfd) out_cfd[q_index] = c;
     out_code[q_index] = reject ? ISSL_CODE_REJECTED : ISSL_CODE_ACCEPTED;
     if (out_count) out_count[q_index] = count;
+}
+
+// Decisions within the reference's rounding. The reference adds a guide's contributions one at a
+// time in double precision, in slice order then list order (:294-296, :362), tests its early exit
+// after every addition (:366-395) and applies the accept rule to the sums where it stopped. The
+// scorers below add the same contributions (the same rounded products) exactly, so an exact total
+// S differs from the reference's running sum over the same hits only by the reference's own
+// rounding: a sum of k non-negative terms rounded after every addition lies within (k - 1) u S
+// of the exact sum (u = 2^-53; Higham, Accuracy and Stability of Numerical Algorithms, 2nd ed.,
+// section 4.2). The exit tests and the accept rules are monotone in both sums, so a decision
+// taken at both ends of that interval is the reference's when the two agree. When they do not
+// (a threshold within a few ulps of one of the guide's running sums) the guide goes to
+// k_replay, which repeats the reference's additions one by one.
+struct Span {
+    double lo, hi;
+};
+// terms bounds the number of non-zero additions (the occurrence sum: a site with no occurrences
+// adds an exact zero); the 8 extra ulps cover the rounding of the exact total to a double and of
+// this computation
+__device__ __forceinline__ Span ref_span(double s, uint64_t terms) {
+    const double w = s * (static_cast<double>(terms + 8) * 0x1p-52);
+    return Span{fmax(s - w, 0.0), s + w};
+}
+// a guide whose exact running totals reach (m, c) without the exit test firing: does the
+// reference certainly not fire either, and (last) does it certainly take the same decision?
+__device__ __forceinline__ bool settled_without_exit(const ScoreParams& P, double m, double c, uint64_t terms,
+                                                     bool last) {
+    const Span sm = ref_span(m, terms), sc = ref_span(c, terms);
+    if (exit_test(P, sm.hi, sc.hi)) return false;
+    return !last || rejects(P, sm.lo, sc.lo) == rejects(P, sm.hi, sc.hi);
+}
+// a guide whose exact totals first fire the exit test at a hit, (pm, pc) before it and (m, c)
+// with it: does the reference certainly stop at the same hit and take the same decision?
+__device__ __forceinline__ bool settled_at_exit(const ScoreParams& P, double pm, double pc, double m, double c,
+                                                uint64_t terms) {
+    const Span bm = ref_span(pm, terms), bc = ref_span(pc, terms);
+    const Span sm = ref_span(m, terms), sc = ref_span(c, terms);
+    return !exit_test(P, bm.hi, bc.hi) && exit_test(P, sm.lo, sc.lo) &&
+           rejects(P, sm.lo, sc.lo) == rejects(P, sm.hi, sc.hi);
 }
 
 __device__ __forceinline__ double warp_incl_sum(double v, int lane) {
@@ -963,6 +1010,7 @@ struct ScoreArgs {
     Counters* counters;
     uint32_t* big;
     uint32_t* exitq;
+    uint32_t* replay;        // guides left to k_replay
     uint32_t* bitmap;
     uint64_t n;
     const uint32_t* d_n;     // batch form: guide count on the device
@@ -1004,6 +1052,12 @@ __device__ __forceinline__ Fx fx_add(Fx a, Fx b) {
     Fx r;
     r.lo = a.lo + b.lo;
     r.hi = a.hi + b.hi + (r.lo < a.lo ? 1ull : 0ull);
+    return r;
+}
+__device__ __forceinline__ Fx fx_sub(Fx a, Fx b) {
+    Fx r;
+    r.lo = a.lo - b.lo;
+    r.hi = a.hi - b.hi - (a.lo < b.lo ? 1ull : 0ull);
     return r;
 }
 __device__ __forceinline__ double fx_double(Fx a) {
@@ -1079,13 +1133,19 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
             tc = fx_add(tc, pr.cfd);
             tn += pr.occ;
         }
-        if (exit_test(P, fx_double(tm), fx_double(tc))) {
+        const double dm = fx_double(tm), dc = fx_double(tc);
+        if (exit_test(P, dm, dc)) {
             if (lane == 0) {
                 if (L <= static_cast<uint32_t>(kWarpSort))
                     a.exitq[atomicAdd(&a.counters->n_exit, 1u)] = static_cast<uint32_t>(qi);
                 else
                     a.big[atomicAdd(&a.counters->n_big, 1u)] = static_cast<uint32_t>(qi);
             }
+            continue;
+        }
+        // within the reference's rounding of the exit test or (last wave) of the accept rule
+        if (!settled_without_exit(P, dm, dc, tn, a.last_wave)) {
+            if (lane == 0) a.replay[atomicAdd(&a.counters->n_replay, 1u)] = static_cast<uint32_t>(qi);
             continue;
         }
         if (P.want_distinct)
@@ -1095,7 +1155,7 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
             }
         if (lane == 0) {
             if (a.last_wave) {
-                finalise(P, fx_double(tm), fx_double(tc), tn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+                finalise(P, dm, dc, tn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
             } else {
                 a.acc[qi] = Acc{tm, tc, tn};
                 a.next_active[atomicAdd(a.d_nnext, 1u)] = static_cast<uint32_t>(qi);
@@ -1193,74 +1253,79 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             cc = Fx{__shfl_sync(0xffffffffu, ic.hi, 31), __shfl_sync(0xffffffffu, ic.lo, 31)};
             cn = __shfl_sync(0xffffffffu, in, 31);
         }
-        if (exit_sl < 0) {  // the totals did not fire after all: every hit counts
-            if (P.want_distinct)
-                for (uint32_t j = lane; j < L; j += 32) {
-                    const uint32_t id = seg[j].r.z;
-                    if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
-                }
-            if (lane == 0) finalise(P, fx_double(cm), fx_double(cc), cn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+        if (exit_sl < 0) {
+            // no slice end fires (k_score_sum fired on the same exact totals, so this does not
+            // happen): the one-by-one rescoring settles it
+            if (lane == 0) a.replay[atomicAdd(&a.counters->n_replay, 1u)] = static_cast<uint32_t>(qi);
             __syncwarp();
             continue;
         }
         const uint32_t b0 = W.cnt[exit_sl], ns = W.cnt[exit_sl + 1] - b0;
-        if (P.want_distinct)  // the sites of the slices before the exit slice
+        rm = bm;
+        rc = bc;
+        rn = bn;
+        // the test fires inside this slice: order its hits by list position
+        uint32_t P2 = 1;
+        while (P2 < ns) P2 <<= 1;
+        for (uint32_t j = lane; j < P2; j += 32)
+            W.keys[j] = j < ns ? (static_cast<uint64_t>(seg[W.idx[b0 + j]].r.x) << 10) | W.idx[b0 + j] : ~0ull;
+        __syncwarp();
+        for (uint32_t k = 2; k <= P2; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = lane; i < P2; i += 32) {
+                    // first stage of each merge compares mirrored pairs, later stages i / i+j
+                    const uint32_t partner = (j == (k >> 1)) ? (i ^ (k - 1)) : (i ^ j);
+                    if (partner > i) {
+                        const uint64_t x = W.keys[i], y = W.keys[partner];
+                        if (x > y) {
+                            W.keys[i] = y;
+                            W.keys[partner] = x;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        // the hit where the exact totals fire: its totals (rm, rc, rn) and those before it (pm, pc)
+        Fx pm = rm, pc = rc;
+        uint32_t stop = ns;
+        for (uint32_t c0 = 0; c0 < ns && stop == ns; c0 += 32) {
+            const uint32_t t = c0 + lane;
+            FxContribution c{{0, 0}, {0, 0}, 0};
+            if (t < ns) c = fx_contribution(P, seg[W.keys[t] & 1023u]);
+            const Fx im = fx_add(fx_warp_incl(c.mit, lane), rm);
+            const Fx ic = fx_add(fx_warp_incl(c.cfd, lane), rc);
+            const uint64_t in = warp_incl_sum_u64(c.occ, lane) + rn;
+            const bool ex = t < ns && exit_test(P, fx_double(im), fx_double(ic));
+            const unsigned em = __ballot_sync(0xffffffffu, ex);
+            const int last = em ? __ffs(em) - 1 : (ns - c0 >= 32 ? 31 : static_cast<int>(ns - c0 - 1));
+            const Fx em_ = fx_sub(im, c.mit), ec_ = fx_sub(ic, c.cfd);
+            if (em) {
+                pm = Fx{__shfl_sync(0xffffffffu, em_.hi, last), __shfl_sync(0xffffffffu, em_.lo, last)};
+                pc = Fx{__shfl_sync(0xffffffffu, ec_.hi, last), __shfl_sync(0xffffffffu, ec_.lo, last)};
+                stop = c0 + last;
+            }
+            rm = Fx{__shfl_sync(0xffffffffu, im.hi, last), __shfl_sync(0xffffffffu, im.lo, last)};
+            rc = Fx{__shfl_sync(0xffffffffu, ic.hi, last), __shfl_sync(0xffffffffu, ic.lo, last)};
+            rn = __shfl_sync(0xffffffffu, in, last);
+        }
+        const double dm = fx_double(rm), dc = fx_double(rc);
+        if (stop == ns || !settled_at_exit(P, fx_double(pm), fx_double(pc), dm, dc, rn)) {
+            if (lane == 0) a.replay[atomicAdd(&a.counters->n_replay, 1u)] = static_cast<uint32_t>(qi);
+            __syncwarp();
+            continue;
+        }
+        if (P.want_distinct) {  // the sites of the slices before the exit slice, then up to the stop
             for (uint32_t j = lane; j < b0; j += 32) {
                 const uint32_t id = seg[W.idx[j]].r.z;
                 if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
-        rm = bm;
-        rc = bc;
-        rn = bn;
-        bool stopped = false;
-        {
-            // the test fires inside this slice: order its hits by list position
-            uint32_t P2 = 1;
-            while (P2 < ns) P2 <<= 1;
-            for (uint32_t j = lane; j < P2; j += 32)
-                W.keys[j] = j < ns ? (static_cast<uint64_t>(seg[W.idx[b0 + j]].r.x) << 10) | W.idx[b0 + j] : ~0ull;
-            __syncwarp();
-            for (uint32_t k = 2; k <= P2; k <<= 1) {
-                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                    for (uint32_t i = lane; i < P2; i += 32) {
-                        // first stage of each merge compares mirrored pairs, later stages i / i+j
-                        const uint32_t partner = (j == (k >> 1)) ? (i ^ (k - 1)) : (i ^ j);
-                        if (partner > i) {
-                            const uint64_t x = W.keys[i], y = W.keys[partner];
-                            if (x > y) {
-                                W.keys[i] = y;
-                                W.keys[partner] = x;
-                            }
-                        }
-                    }
-                    __syncwarp();
-                }
+            for (uint32_t j = lane; j <= stop; j += 32) {
+                const uint32_t id = seg[W.keys[j] & 1023u].r.z;
+                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
-            for (uint32_t c0 = 0; c0 < ns && !stopped; c0 += 32) {
-                const uint32_t t = c0 + lane;
-                FxContribution c{{0, 0}, {0, 0}, 0};
-                uint32_t id = 0;
-                if (t < ns) {
-                    const HitRec hr = seg[W.keys[t] & 1023u];
-                    id = hr.r.z;
-                    c = fx_contribution(P, hr);
-                }
-                const Fx im = fx_add(fx_warp_incl(c.mit, lane), rm);
-                const Fx ic = fx_add(fx_warp_incl(c.cfd, lane), rc);
-                const uint64_t in = warp_incl_sum_u64(c.occ, lane) + rn;
-                const bool ex = t < ns && exit_test(P, fx_double(im), fx_double(ic));
-                const unsigned em = __ballot_sync(0xffffffffu, ex);
-                const int last = em ? __ffs(em) - 1 : (ns - c0 >= 32 ? 31 : static_cast<int>(ns - c0 - 1));
-                if (P.want_distinct && t < ns && lane <= last && id != kNoSite)
-                    atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
-                rm = Fx{__shfl_sync(0xffffffffu, im.hi, last), __shfl_sync(0xffffffffu, im.lo, last)};
-                rc = Fx{__shfl_sync(0xffffffffu, ic.hi, last), __shfl_sync(0xffffffffu, ic.lo, last)};
-                rn = __shfl_sync(0xffffffffu, in, last);
-                stopped = em != 0;
-            }
-            __syncwarp();
         }
-        if (lane == 0) finalise(P, fx_double(rm), fx_double(rc), rn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+        if (lane == 0) finalise(P, dm, dc, rn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
         __syncwarp();
     }
 }
@@ -1322,16 +1387,15 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
                 __syncthreads();
             }
         }
-        bool stopped = false;
-        for (uint32_t c0 = 0; c0 < L && !stopped; c0 += blockDim.x) {
+        // sorted position of the hit where the exact totals fire, and the totals before it
+        uint32_t stop = L;
+        Fx pre_m = run_m, pre_c = run_c;
+        for (uint32_t c0 = 0; c0 < L && stop == L; c0 += blockDim.x) {
             const uint32_t t = c0 + threadIdx.x;
             FxContribution c{{0, 0}, {0, 0}, 0};
-            uint32_t id = 0;
             if (t < L) {
                 const uint32_t h = in_smem ? static_cast<uint32_t>(s_bkeys[t] & ((1u << kBlockIdxBits) - 1)) : t;
-                const HitRec hr = seg[h];
-                id = hr.r.z;
-                c = fx_contribution(P, hr);
+                c = fx_contribution(P, seg[h]);
             }
             Fx im = fx_warp_incl(c.mit, lane), ic = fx_warp_incl(c.cfd, lane);
             uint64_t in = warp_incl_sum_u64(c.occ, lane);
@@ -1357,24 +1421,127 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             const int first = s_first;
             const uint32_t in_chunk = L - c0 < blockDim.x ? L - c0 : blockDim.x;
             const int last = first != 0x7fffffff ? first : static_cast<int>(in_chunk) - 1;
-            if (P.want_distinct && t < L && static_cast<int>(threadIdx.x) <= last)
-                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             __syncthreads();
             if (static_cast<int>(threadIdx.x) == last) {
                 s_wm[0] = im;
                 s_wc[0] = ic;
                 s_wn[0] = in;
+                s_wm[1] = fx_sub(im, c.mit);
+                s_wc[1] = fx_sub(ic, c.cfd);
             }
             __syncthreads();
             run_m = s_wm[0];
             run_c = s_wc[0];
             run_n = s_wn[0];
-            stopped = first != 0x7fffffff;
+            if (first != 0x7fffffff) {
+                pre_m = s_wm[1];
+                pre_c = s_wc[1];
+                stop = c0 + static_cast<uint32_t>(first);
+            }
             __syncthreads();
         }
-        if (threadIdx.x == 0)
-            finalise(P, fx_double(run_m), fx_double(run_c), run_n, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+        const double dm = fx_double(run_m), dc = fx_double(run_c);
+        if (stop == L || !settled_at_exit(P, fx_double(pre_m), fx_double(pre_c), dm, dc, run_n)) {
+            // within the reference's rounding (or, which does not happen, no hit fires)
+            if (threadIdx.x == 0) a.replay[atomicAdd(&a.counters->n_replay, 1u)] = static_cast<uint32_t>(qi);
+            __syncthreads();
+            continue;
+        }
+        if (P.want_distinct)
+            for (uint32_t t = threadIdx.x; t <= stop; t += blockDim.x) {
+                const uint32_t h = in_smem ? static_cast<uint32_t>(s_bkeys[t] & ((1u << kBlockIdxBits) - 1)) : t;
+                const uint32_t id = seg[h].r.z;
+                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+            }
+        if (threadIdx.x == 0) finalise(P, dm, dc, run_n, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
         __syncthreads();
+    }
+}
+
+// Warp per guide that the exact totals cannot settle (see settled_at_exit): the reference's
+// additions repeated one at a time, in its order -- slices in order, each bucket in list order,
+// sites an earlier slice reached skipped (the ownership rule; the reference's toggle bitset,
+// :252-258) -- with its early-exit test after every addition (:366-395), straight from the index.
+// Such guides are rare (a threshold within a few ulps of one of their running sums), so this
+// favours plainness over speed: the lanes compare 32 blocks of a bucket at once, then the warp
+// walks their owned sites in list order, every lane doing the same additions.
+__global__ void __launch_bounds__(256) k_replay(ScoreArgs a, IndexView v) {
+    __shared__ SliceGeom g[kMaxSlices];
+    for (int i = threadIdx.x; i < static_cast<int>(v.n_slices); i += blockDim.x) g[i] = v.geom[i];
+    __syncthreads();
+    if (a.counters->overflow) return;  // rerun follows
+    const int lane = threadIdx.x & 31;
+    const uint32_t n = a.counters->n_replay;
+    const Tables& T = *a.tables;
+    for (uint32_t e = blockIdx.x * 8u + (threadIdx.x >> 5); e < n; e += gridDim.x * 8u) {
+        const uint64_t qi = a.replay[e];
+        const ScoreParams P = params_of(a, qi);
+        const uint64_t q = a.qsig[qi];
+        double tm = 0.0, tc = 0.0;
+        uint64_t cnt = 0;
+        bool stop = false;
+        for (uint32_t s = 0; s < v.n_slices && !stop; s++) {
+            const SliceGeom& G = g[s];
+            const uint64_t gb = G.bbase + slice_key(q, G), base = static_cast<uint64_t>(s) * v.n_sites;
+            const uint64_t e0 = v.offsets[gb] - base, e1 = v.offsets[gb + 1] - base;
+            if (e1 <= e0) continue;
+            const uint32_t rq = slice_residual(q, G);
+            for (uint64_t b0 = e0 / 32; b0 <= (e1 - 1) / 32 && !stop; b0 += 32) {
+                const uint64_t b = b0 + lane;
+                uint32_t own = 0;
+                if (b <= (e1 - 1) / 32) {
+                    const uint32_t* blk = v.rbits + (G.wbase + b * G.wpb - v.rbits_base);
+                    uint32_t mm[kSeqLen];  // mismatch word of each residual position
+                    uint32_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;  // saturating bit-sliced count
+                    for (int p = 0; p < G.rwidth; p++) {
+                        const uint32_t q0 = 0u - ((rq >> (2 * p)) & 1u), q1 = 0u - ((rq >> (2 * p + 1)) & 1u);
+                        const uint32_t m = (blk[2 * p] ^ q0) | (blk[2 * p + 1] ^ q1);
+                        mm[p] = m;
+                        const uint32_t k0 = c0 & m;
+                        c0 ^= m;
+                        const uint32_t k1 = c1 & k0;
+                        c1 ^= k0;
+                        const uint32_t k2 = c2 & k1;
+                        c2 ^= k1;
+                        c3 |= k2;
+                    }
+                    const int64_t lo = static_cast<int64_t>(e0) - static_cast<int64_t>(32 * b);
+                    const int64_t hi = static_cast<int64_t>(e1) - static_cast<int64_t>(32 * b);
+                    const uint32_t valid = (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & (lo <= 0 ? 0xFFFFFFFFu : ~((1u << lo) - 1u));
+                    uint32_t cb = bs::within(bs::Count{c0, c1, c2, c3}, P.max_dist) & valid;
+                    while (cb) {
+                        const int k = __ffs(cb) - 1;
+                        cb &= cb - 1;
+                        uint32_t mism20 = 0;
+                        for (int p = 0; p < G.rwidth; p++)
+                            if ((mm[p] >> k) & 1u) mism20 |= 1u << G.rpos[p];
+                        bool owned = true;
+                        for (uint32_t t = 0; t < s && owned; t++) owned = (mism20 & g[t].pmask) != 0;
+                        if (owned) own |= 1u << k;
+                    }
+                }
+                for (int l = 0; l < 32 && !stop; l++) {
+                    uint32_t ob = __shfl_sync(0xffffffffu, own, l);
+                    while (ob && !stop) {
+                        const int k = __ffs(ob) - 1;
+                        ob &= ob - 1;
+                        const uint32_t pos = static_cast<uint32_t>(32 * (b0 + l) + k);
+                        uint32_t id, occ;
+                        uint64_t sig;
+                        load_site(v, s, pos, q, G, id, occ, sig);
+                        const Contribution c = contribution(T, P, q, sig, occ);
+                        if (c.dist > P.max_dist) continue;  // not scored (:292)
+                        tm = __dadd_rn(tm, c.mit);
+                        tc = __dadd_rn(tc, c.cfd);
+                        cnt += occ;
+                        if (P.want_distinct && lane == 0) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                        stop = exit_test(P, tm, tc);
+                    }
+                }
+            }
+        }
+        if (lane == 0) finalise(P, tm, tc, cnt, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
+        __syncwarp();
     }
 }
 
@@ -1406,20 +1573,29 @@ int sm_count(int device) {
     return v > 0 ? v : 148;
 }
 
+// The penalty tables as the kernels read them: MIT by subset rank, CFD position and PAM penalties,
+// and the binomial coefficients of the MIT rank. Every device copy is made from this one image.
+const Tables& host_tables() {
+    static const Tables h = [] {
+        Tables t;
+        const auto& mit = mit_rank_table();
+        std::memcpy(t.mit, mit.data(), sizeof t.mit);
+        std::memcpy(t.cfd_pos, cfd_pos_table(), sizeof t.cfd_pos);
+        std::memcpy(t.cfd_pam, cfd_pam_table(), sizeof t.cfd_pam);
+        for (int p = 0; p < 20; p++)
+            for (int i = 0; i < 5; i++) {
+                uint64_t r = (i <= p) ? 1 : 0;
+                for (int k = 1; k <= i && i <= p; k++) r = r * (p - i + k) / k;
+                t.binom[p][i] = static_cast<uint32_t>(r);
+            }
+        return t;
+    }();
+    return h;
+}
+
 void init_tables(Workspace& ws, cudaStream_t st) {
-    Tables h;
-    const auto& mit = mit_rank_table();
-    std::memcpy(h.mit, mit.data(), sizeof h.mit);
-    std::memcpy(h.cfd_pos, cfd_pos_table(), sizeof h.cfd_pos);
-    std::memcpy(h.cfd_pam, cfd_pam_table(), sizeof h.cfd_pam);
-    for (int p = 0; p < 20; p++)
-        for (int i = 0; i < 5; i++) {
-            uint64_t r = (i <= p) ? 1 : 0;
-            for (int t = 1; t <= i && i <= p; t++) r = r * (p - i + t) / t;
-            h.binom[p][i] = static_cast<uint32_t>(r);
-        }
     ws.tables.reserve(1);
-    ISSL_CUDA(cudaMemcpyAsync(ws.tables.p, &h, sizeof h, cudaMemcpyHostToDevice, st));
+    ISSL_CUDA(cudaMemcpyAsync(ws.tables.p, &host_tables(), sizeof(Tables), cudaMemcpyHostToDevice, st));
     ISSL_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -1580,6 +1756,7 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
         ws.qhoff.reserve(cap + 1);
         ws.big.reserve(cap);
         ws.exitq.reserve(cap);
+        ws.replayq.reserve(cap);
         ws.out_mit.reserve(cap);
         ws.out_cfd.reserve(cap);
         ws.out_code.reserve(cap);
@@ -1639,9 +1816,9 @@ void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide,
     *per_candidate = kCandSlotBytes;
     *fixed = 12 * (G + 1) + sizeof(Tables) + sizeof(Counters) + (kScanBlocks + 4) * 12 + 4096 * sizeof(UnitDesc) +
              (65536 + slab_slack) * *per_candidate;
-    // qsig, probe lists, hit counts and offsets, exit queues, outputs, set map, wave lists and
-    // running totals; scan units
-    *per_guide = 8 + 12 * S + 4 * 4 + (8 + 8 + 1 + 8) + 2 + 2 * 4 + 5 * 8 +
+    // qsig, probe lists, hit counts and offsets, exit and replay queues, outputs, set map, wave
+    // lists and running totals; scan units
+    *per_guide = 8 + 12 * S + 5 * 4 + (8 + 8 + 1 + 8) + 2 + 2 * 4 + 5 * 8 +
                  sizeof(UnitDesc) * 3 * S * (kChunk / min_chunk);
     uint64_t idw, cw;  // the two slice windows of a host-list index
     window_capacity(ix, &idw, &cw);
@@ -1811,6 +1988,7 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         a.qsig = R.qsig;
         a.seg = ws.seg.p;
         a.exitq = ws.exitq.p;
+        a.replay = ws.replayq.p;
         a.qhoff = ws.qhoff.p;
         a.tables = ws.tables.p;
         a.counters = C;
@@ -1836,6 +2014,21 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         k_score_ordered<<<sms * 4, 256, 8 * sizeof(OrderedSmem), st>>>(a);
         k_score_block<<<sms * 2, 256, kBlockHits * sizeof(uint64_t), st>>>(a);
         k += 3;
+        if (last) {
+            // guides the exact totals do not settle, rescored one addition at a time from the
+            // whole index (a host-list index: its lists read in place from page-locked host memory)
+            IndexView vr = v0;
+            if (staged) {
+                void* d_ids = nullptr;
+                void* d_rbits = nullptr;
+                ISSL_CUDA(cudaHostGetDevicePointer(&d_ids, ix->h_ids.p, 0));
+                ISSL_CUDA(cudaHostGetDevicePointer(&d_rbits, ix->h_rbits.p, 0));
+                vr.ids = static_cast<const uint32_t*>(d_ids);
+                vr.rbits = static_cast<const uint32_t*>(d_rbits);
+            }
+            k_replay<<<sms, 256, 0, st>>>(a, vr);
+            k++;
+        }
     }
     if (R.P.want_distinct && R.distinct_last) {
         k_popcount<<<sms * 4, 256, 0, st>>>(ws.bitmap.p, ix->n_sites / 32 + 1, C);
@@ -1855,6 +2048,13 @@ bool check_and_grow(Workspace& ws, cudaStream_t st) {
     if (c.overflow & 4u) {
         ws.zero_state_ok = false;
         throw Error(ISSL_ERR_TIMEOUT, "scan: an asynchronous copy did not complete within the wait limit");
+    }
+    if (c.dropped) {
+        // a grouped hit farther than four mismatches from its guide: a candidate record that does
+        // not describe a site of the guide's bucket. Never silently: the call's results are void.
+        ws.zero_state_ok = false;
+        throw Error(ISSL_ERR_INTERNAL, "scoring: " + std::to_string(c.dropped) +
+                                           " candidate sites were farther than 4 mismatches from their guide");
     }
     const uint64_t units = c.max_units;
     bool ok = true;
@@ -1899,6 +2099,7 @@ void fill_stats(const Workspace& ws, float scan_ms, float total_ms, uint64_t lau
     s.candidates = ws.last.cands;
     s.staged_bytes = ws.staged;
     s.dropped_hits = ws.last.dropped;
+    s.replayed = ws.last.n_replay;
 }
 
 issl_score_stats run_stats(issl_index* ix, Workspace& ws) {
@@ -1930,6 +2131,7 @@ void add_stats(issl_score_stats& a, const issl_score_stats& b) {
     a.candidates += b.candidates;
     a.staged_bytes += b.staged_bytes;
     a.dropped_hits += b.dropped_hits;
+    a.replayed += b.replayed;
 }
 
 // One pipeline run over n guides, growing the workspace and rerunning on overflow.
@@ -2429,18 +2631,18 @@ int issl_last_stats(const issl_index* ix, issl_score_stats* out) {
 // =============================================================================================
 // Allocation-free scoring.
 //
-// Some callers cannot allocate device memory when they score: code that runs while a stream is
-// being captured into a CUDA graph, hosts that hand all device memory to their own pool
-// allocator (a framework's caching allocator, a fixed arena on a shared GPU) and forbid stray
-// cudaMalloc calls, and latency-bound services that allow no allocation after start-up. The
-// regular entry points grow a per-index workspace on demand; issl_score_device_static instead
-// runs one kernel whose only scratch is the file-scope array below, fixed at library load.
+// Some callers cannot allocate device memory when they score: hosts that hand all device memory
+// to their own pool allocator (a framework's caching allocator, a fixed arena on a shared GPU)
+// and forbid stray cudaMalloc calls, and latency-bound services that allow no allocation after
+// start-up. The regular entry points grow a per-index workspace on demand;
+// issl_score_device_static instead runs one kernel whose only scratch is the file-scope array
+// below, fixed at library load.
 //
 // One block scores one guide at a time (grid-stride over the guides): for every slice it walks
 // the guide's bucket block by block with the bit-sliced comparison, applies the ownership rule
 // to each candidate, stores the owned hits of the guide in its block's slice of g_static_hits,
-// sorts them in shared memory in the order the reference visits them, and accumulates MIT and
-// CFD with the reference's early exit.
+// sorts them in shared memory in the order the reference visits them, and adds their MIT and
+// CFD contributions one at a time in that order with the reference's early exit.
 // =============================================================================================
 namespace issl {
 namespace {
@@ -2482,8 +2684,9 @@ __device__ __forceinline__ void static_block(const StaticArgs& a, const SliceGeo
     uint32_t mm[RW];
 #pragma unroll
     for (int p = 0; p < RW; p++) mm[p] = (blk[2 * p] ^ qm[2 * p]) | (blk[2 * p + 1] ^ qm[2 * p + 1]);
-    const int lo = max(static_cast<int>(e0) - static_cast<int>(32 * b), 0);
-    const int hi = min(static_cast<int>(e1) - static_cast<int>(32 * b), 32);
+    // the bucket's positions in this block (list positions can exceed 2^31: 64-bit differences)
+    const int64_t lo = max(static_cast<int64_t>(e0) - static_cast<int64_t>(32 * b), int64_t{0});
+    const int64_t hi = min(static_cast<int64_t>(e1) - static_cast<int64_t>(32 * b), int64_t{32});
     const uint32_t valid = (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
     uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), a.P.max_dist) & valid;
     while (cbits) {
@@ -2511,9 +2714,9 @@ __global__ void __launch_bounds__(kStaticThreads) k_score_static(StaticArgs a) {
     __shared__ SliceGeom s_geom[kMaxSlices];
     __shared__ uint32_t s_qm[32];
     __shared__ uint32_t s_cnt;
-    __shared__ double s_wm[kStaticThreads / 32], s_wc[kStaticThreads / 32];
-    __shared__ uint64_t s_wn[kStaticThreads / 32];
-    __shared__ int s_first;
+    __shared__ double s_cm[kStaticThreads], s_cc[kStaticThreads];
+    __shared__ uint32_t s_co[kStaticThreads];
+    __shared__ int s_stop;
     for (int i = threadIdx.x; i < static_cast<int>(a.ix.n_slices); i += blockDim.x) s_geom[i] = a.ix.geom[i];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -2577,54 +2780,36 @@ __global__ void __launch_bounds__(kStaticThreads) k_score_static(StaticArgs a) {
                 __syncthreads();
             }
         }
+        // the reference's additions, one at a time in that order (thread 0), with its early-exit
+        // test after each (:366-395); the block computes the contributions 256 at a time
         double run_mit = 0.0, run_cfd = 0.0;
         uint64_t run_cnt = 0;
         bool stopped = false;
         for (uint32_t c0 = 0; c0 < L && !stopped; c0 += blockDim.x) {
             const uint32_t t = c0 + threadIdx.x;
-            Contribution c{0.0, 0.0, 0};
             if (t < L) {
                 const uint4 r = hits[s_keys[t] & (kStaticHits - 1)];
                 uint32_t id, occ;
                 uint64_t sig;
                 load_site(a.ix, r.y, r.x, q, s_geom[r.y], id, occ, sig);
-                c = contribution(T, a.P, q, sig, occ);
-            }
-            double im = warp_incl_sum(c.mit, lane), ic = warp_incl_sum(c.cfd, lane);
-            uint64_t in = warp_incl_sum_u64(c.occ, lane);
-            if (lane == 31) {
-                s_wm[warp] = im;
-                s_wc[warp] = ic;
-                s_wn[warp] = in;
-            }
-            if (threadIdx.x == 0) s_first = 0x7fffffff;
-            __syncthreads();
-            double pm = run_mit, pc = run_cfd;
-            uint64_t pn = run_cnt;
-            for (int w = 0; w < warp; w++) {
-                pm += s_wm[w];
-                pc += s_wc[w];
-                pn += s_wn[w];
-            }
-            im += pm;
-            ic += pc;
-            in += pn;
-            if (t < L && exit_test(a.P, im, ic)) atomicMin(&s_first, static_cast<int>(threadIdx.x));
-            __syncthreads();
-            const int first = s_first;
-            const uint32_t in_chunk = L - c0 < blockDim.x ? L - c0 : blockDim.x;
-            const int last = first != 0x7fffffff ? first : static_cast<int>(in_chunk) - 1;
-            __syncthreads();
-            if (static_cast<int>(threadIdx.x) == last) {
-                s_wm[0] = im;
-                s_wc[0] = ic;
-                s_wn[0] = in;
+                const Contribution c = contribution(T, a.P, q, sig, occ);
+                s_cm[threadIdx.x] = c.mit;
+                s_cc[threadIdx.x] = c.cfd;
+                s_co[threadIdx.x] = occ;
             }
             __syncthreads();
-            run_mit = s_wm[0];
-            run_cfd = s_wc[0];
-            run_cnt = s_wn[0];
-            stopped = first != 0x7fffffff;
+            if (threadIdx.x == 0) {
+                const uint32_t m = L - c0 < blockDim.x ? L - c0 : blockDim.x;
+                for (uint32_t i = 0; i < m && !stopped; i++) {
+                    run_mit = __dadd_rn(run_mit, s_cm[i]);
+                    run_cfd = __dadd_rn(run_cfd, s_cc[i]);
+                    run_cnt += s_co[i];
+                    stopped = exit_test(a.P, run_mit, run_cfd);
+                }
+                s_stop = stopped;
+            }
+            __syncthreads();
+            stopped = s_stop != 0;
             __syncthreads();
         }
         if (threadIdx.x == 0)
@@ -2652,18 +2837,7 @@ StaticScratch& static_scratch(int device) {
         ISSL_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.hits), g_static_hits));
         ISSL_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.status), g_static_status));
         ISSL_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.tables), g_static_tables));
-        Tables h;
-        const auto& mit = mit_rank_table();
-        std::memcpy(h.mit, mit.data(), sizeof h.mit);
-        std::memcpy(h.cfd_pos, cfd_pos_table(), sizeof h.cfd_pos);
-        std::memcpy(h.cfd_pam, cfd_pam_table(), sizeof h.cfd_pam);
-        for (int p = 0; p < 20; p++)
-            for (int i = 0; i < 5; i++) {
-                uint64_t r = (i <= p) ? 1 : 0;
-                for (int t = 1; t <= i && i <= p; t++) r = r * (p - i + t) / t;
-                h.binom[p][i] = static_cast<uint32_t>(r);
-            }
-        ISSL_CUDA(cudaMemcpy(sc.tables, &h, sizeof h, cudaMemcpyHostToDevice));
+        ISSL_CUDA(cudaMemcpy(sc.tables, &host_tables(), sizeof(Tables), cudaMemcpyHostToDevice));
         sc.ready = true;
     }
     return sc;

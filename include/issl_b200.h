@@ -31,6 +31,8 @@ extern "C" {
 #define ISSL_ERR_TIMEOUT (-6)     /* a bounded device wait gave up */
 #define ISSL_ERR_UNSUPPORTED (-7) /* valid request this build does not implement */
 #define ISSL_ERR_BUSY (-8)        /* admission refused: not enough device memory now */
+#define ISSL_ERR_INTERNAL (-9)    /* a consistency check of the pipeline failed; the call's
+                                     outputs are not valid (message says which check) */
 
 /* ---- score methods: otScoreMethod, include/util.hpp:20 (same numbering) -------------- */
 #define ISSL_METHOD_MIT 0
@@ -140,16 +142,17 @@ int issl_score_device(issl_index* index, const uint64_t* d_sigs, size_t n, int m
 
 /* Allocation-free scoring. No counterpart in the reference, which scores on the CPU.
  *
- * For callers that cannot allocate device memory while they score: code running during CUDA
- * graph capture, hosts whose device memory belongs to their own pool allocator, services that
- * allow no allocation after start-up. The regular entry points grow a per-index workspace on
- * demand; this one allocates nothing (no cudaMalloc, no cudaFree, no allocating library call).
- * Its only scratch is a fixed 9.7 MB array inside the library, which every GPU that loads the
- * library holds until the process exits.
+ * For callers that cannot allocate device memory while they score: hosts whose device memory
+ * belongs to their own pool allocator (a framework's caching allocator, a fixed arena on a shared
+ * GPU) and forbid stray cudaMalloc calls, and services that allow no allocation after start-up.
+ * The regular entry points grow a per-index workspace on demand; this one allocates nothing (no
+ * cudaMalloc, no cudaFree, no allocating library call). Its only scratch is a fixed 9.7 MB array
+ * inside the library, which every GPU that loads the library holds until the process exits.
  *
  * Same arguments and results as issl_score_device (minus the distinct count), buffers in device
  * memory of the index's device, enqueued on `stream` (NULL = the default stream); the call waits
- * for the kernel to finish. Limits: at most ISSL_STATIC_MAX_GUIDES guides per call (larger n is
+ * for the kernel to finish, then reads the overflow flag. Each guide's sums are accumulated one
+ * addition at a time in the reference's order, as the reference does. Limits: at most ISSL_STATIC_MAX_GUIDES guides per call (larger n is
  * rejected with ISSL_ERR_ARG) and at most ISSL_STATIC_MAX_HITS owned off-target hits per guide
  * (a guide beyond that makes the call fail with ISSL_ERR_UNSUPPORTED; its outputs are not set).
  * The first call on a device looks up the scratch address and uploads the penalty tables; make
@@ -172,8 +175,11 @@ typedef struct {
     uint64_t class_probes[3];   /* probes into buckets of < 64, 64..4095 and >= 4096 entries */
     uint64_t candidates;        /* candidate slots the scan wrote, before the ownership rule */
     uint64_t staged_bytes;      /* host-list index: list bytes copied from host memory */
-    uint64_t dropped_hits;      /* candidate sites found farther than 4 mismatches from their guide
-                                   (none by construction; counted for nothing if ever seen) */
+    uint64_t dropped_hits;      /* candidate sites found farther than 4 mismatches from their guide:
+                                   none by construction; any makes the call fail with
+                                   ISSL_ERR_INTERNAL */
+    uint64_t replayed;          /* guides whose decision lay within the reference's rounding of
+                                   its running sums, rescored one addition at a time */
 } issl_score_stats;
 
 /* Frees the device memory of the index's own scoring workspace (the buffers the plain

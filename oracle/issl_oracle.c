@@ -353,6 +353,47 @@ int ora_score(const ora_index* idx, const uint64_t* qsigs, uint64_t nq, int meth
     return err;
 }
 
+/* The terms one guide's sums receive, in the order the reference adds them (slices in order,
+ * each bucket in list order, sites seen in an earlier slice skipped; lib/ISSLScoringModule.cpp
+ * :230-363) with no early exit: for every scored site (dist <= max_dist) its MIT term
+ * (score * occurrences, 0 for an exact match, :294-298), its CFD term (:301-362) and its
+ * occurrences. Returns the number of scored sites; at most cap are written. */
+uint64_t ora_trace(const ora_index* idx, uint64_t q, int max_dist, double* mit_terms, double* cfd_terms,
+                   uint32_t* occ_out, uint64_t cap) {
+    build_mit20();
+    const uint64_t N = idx->n_sites, S = idx->n_slices;
+    uint64_t pos[64];
+    uint64_t base = 0, n = 0;
+    uint64_t* seen = calloc(N / 64 + 1, 8);
+    for (uint64_t s = 0; s < S; s++) {
+        const int w = mask_positions(idx->slice_masks[s], idx->seq_len, pos);
+        uint64_t key = 0;
+        for (int j = 0; j < w; j++) key |= ((q >> (pos[j] * 2)) & 3ULL) << (j * 2);
+        uint64_t start = 0;
+        for (uint64_t b = 0; b < key; b++) start += idx->list_sizes[base + b];
+        const uint64_t* lst = idx->lists + s * N + start;
+        for (uint64_t j = 0; j < idx->list_sizes[base + key]; j++) {
+            const uint64_t id = lst[j] & 0xFFFFFFFFULL;
+            const uint32_t occ = (uint32_t)(lst[j] >> 32);
+            if ((seen[id / 64] >> (id % 64)) & 1ULL) continue;
+            seen[id / 64] |= 1ULL << (id % 64);
+            const uint64_t x = q ^ idx->sigs[id];
+            const uint64_t mism = ((x & 0xAAAAAAAAAAAAAAAAULL) >> 1) | (x & 0x5555555555555555ULL);
+            const uint64_t dist = (uint64_t)__builtin_popcountll(mism);
+            if (dist > (uint64_t)max_dist) continue;
+            if (n < cap) {
+                mit_terms[n] = dist > 0 ? g_mit20[compress_even(mism)] * (double)occ : 0.0;
+                cfd_terms[n] = cfd_score(q, idx->sigs[id], dist) * (double)occ;
+                occ_out[n] = occ;
+            }
+            n++;
+        }
+        base += 1ULL << (2 * w);
+    }
+    free(seen);
+    return n;
+}
+
 void ora_finalise(int method, double t, double tot_mit, double tot_cfd, double* mit_score,
                   double* cfd_score, char* code) {
     double m = 10000.0 / (100.0 + tot_mit), c = 10000.0 / (100.0 + tot_cfd);

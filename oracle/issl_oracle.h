@@ -75,6 +75,13 @@ int ora_score(const ora_index* idx, const uint64_t* query_sigs, uint64_t n_queri
               double threshold, int max_dist, int threads, double* tot_mit, double* tot_cfd,
               uint64_t* count, uint64_t* distinct);
 
+/* The scored terms of one guide in the reference's adding order, without the early exit
+ * (lib/ISSLScoringModule.cpp:230-363): MIT term, CFD term and occurrences per scored site.
+ * Returns the number of scored sites (at most cap written). For deriving thresholds that sit
+ * on the reference's own running sums. */
+uint64_t ora_trace(const ora_index* idx, uint64_t query_sig, int max_dist, double* mit_terms,
+                   double* cfd_terms, uint32_t* occ, uint64_t cap);
+
 /* Per-guide finalisation, lib/ISSLScoringModule.cpp:404-459: scores and the accept code
  * ('1' accepted / '0' rejected). For mit (cfd) the unused score is -1. */
 void ora_finalise(int method, double threshold, double tot_mit, double tot_cfd, double* mit_score,

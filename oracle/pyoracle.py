@@ -59,6 +59,9 @@ def lib():
                                    P(C.c_double), C.c_char_p]
         L.ora_bruteforce.argtypes = [P(C.c_uint64), P(C.c_uint32), C.c_uint64, P(C.c_uint64), C.c_uint64,
                                      C.c_int, C.c_int, P(C.c_double), P(C.c_double), P(C.c_uint64)]
+        L.ora_trace.restype = C.c_uint64
+        L.ora_trace.argtypes = [C.POINTER(OraIndex), C.c_uint64, C.c_int, P(C.c_double), P(C.c_double),
+                                P(C.c_uint32), C.c_uint64]
         _lib = L
     return _lib
 
@@ -151,6 +154,17 @@ class Index:
         if rc != 0:
             raise RuntimeError("oracle: MIT table lookup failed (the reference would throw)")
         return mit, cfd, cnt, int(distinct[0])
+
+    def trace(self, qsig: int, max_dist: int = 4):
+        """The scored terms of one guide in the reference's adding order, no early exit:
+        (mit_terms, cfd_terms, occurrences) arrays."""
+        n = int(lib().ora_trace(C.byref(self.s), int(qsig), max_dist, None, None, None, 0))
+        mit = np.zeros(max(n, 1))
+        cfd = np.zeros(max(n, 1))
+        occ = np.zeros(max(n, 1), np.uint32)
+        lib().ora_trace(C.byref(self.s), int(qsig), max_dist, _p(mit, C.c_double), _p(cfd, C.c_double),
+                        _p(occ, C.c_uint32), n)
+        return mit[:n], cfd[:n], occ[:n]
 
     def free(self):
         if self.s.owns_memory:

@@ -54,3 +54,17 @@ def load_case(name):
 
 
 CASE_NAMES = ["c0_small", "c1_small", "c2_small", "c4_small"]
+
+
+def c0_full_index():
+    """Config 0 at its stated size, regenerated from its seed in the reference's site order."""
+    import synth
+    from cracklingplusplus_gpu_b200.slice_configs import slice_masks
+    z, meta = load_case("c0_full")
+    sites, occ, queries = synth.make_case(meta["seed"], meta["n_sites"], meta["n_queries"], repeat_frac=0.0,
+                                          planted_into_sites=True)
+    order = synth.reference_order(sites)
+    occ_of = dict(zip(sites.tolist(), occ.tolist()))
+    occ_sorted = np.array([occ_of[int(s)] for s in order.tolist()], np.uint32)
+    np.testing.assert_array_equal(queries, z["queries"])
+    return z, meta, order, occ_sorted, np.array(slice_masks(meta["config"]), np.uint64)

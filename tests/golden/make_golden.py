@@ -14,6 +14,12 @@ Outputs
                      outputs (ISSLScoringModule::run scores at %.17g and accept codes for every
                      method and threshold; ISSLScoreOfftargets per-query counts and distinct
                      site count)
+  case_knife.npz     thresholds on the reference's own running sums (knife_edge.py), one
+                     (guide, method, threshold) per entry, scored by the same two binaries
+  case_c0_full.npz   config 0 at its stated size (1M sites, slice-4-5, 1,000 guides): outputs
+                     only, the sites are regenerated from the seed
+
+python tests/golden/make_golden.py [names...] regenerates only the named fixtures.
 """
 from __future__ import annotations
 
@@ -32,10 +38,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("ISSL_REFERENCE", "/root/reference")
 REF_BIN = os.path.join(REPO, "oracle", "_ref")
 sys.path.insert(0, HERE)
 sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+from refpath import REFERENCE as REF  # noqa: E402
 
 import synth  # noqa: E402
 from cracklingplusplus_gpu_b200.slice_configs import SLICE_CONFIGS  # noqa: E402
@@ -118,7 +125,8 @@ def ref_cli(index, queries, method_cli, threshold, tmp):
     with open(qp, "w") as f:
         f.write("".join(q + "\n" for q in queries))
     work = tempfile.mkdtemp(dir=tmp)
-    r = run([os.path.join(REF_BIN, "ISSLScoreOfftargets"), index, qp, "4", repr(threshold), method_cli,
+    # the build without FMA contraction: its sums are rounded as the reference's release build rounds them
+    r = run([os.path.join(REF_BIN, "ISSLScoreOfftargets_exact"), index, qp, "4", repr(threshold), method_cli,
              "cli_out.txt"], cwd=work)
     out_files = [p for p in glob.glob(os.path.join(work, "*")) if p.endswith("cli_out.txt") and os.path.isfile(p)]
     assert len(out_files) == 1, out_files
@@ -219,6 +227,104 @@ def make_tiny(tmp):
     print(f"tiny: {len(sites)} sites, {len(queries)} queries")
 
 
+KNIFE = {"name": "knife", "seed": 15, "n_sites": 40000, "n_queries": 400, "config": "slice-8-20",
+         "repeat_frac": 0.3, "n_seeds": 30, "repeat_query_frac": 0.5, "guides": 24, "min_hits": 20}
+
+
+def _oracle(pen_pos, pen_pam):
+    import pyoracle
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle")], check=True)
+    pyoracle.set_cfd_tables(pen_pos, pen_pam)
+    return pyoracle
+
+
+def make_knife(tmp, pen_pos, pen_pam):
+    """Thresholds on the reference's own running sums (knife_edge.py): per selected guide and
+    method, thresholds whose maximum_sum is within a few ulps of the rounded running quantity at
+    the last hit and at an interior hit, and every threshold between the rounded and the exactly
+    summed quantity. Each (guide, method, threshold) is scored by the reference module and CLI."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import knife_edge
+    K = KNIFE
+    sites, occ, queries = synth.make_case(K["seed"], K["n_sites"], K["n_queries"], repeat_frac=K["repeat_frac"],
+                                          n_seeds=K["n_seeds"], planted_into_sites=False,
+                                          repeat_query_frac=K["repeat_query_frac"])
+    idx_path = os.path.join(tmp, "knife.issl")
+    sorted_seqs = ref_build_index(sites, occ, SLICE_CONFIGS[K["config"]], idx_path, tmp)
+    sig_sorted = np.array([synth.seq_to_sig(x) for x in sorted_seqs], np.uint64)
+    occ_map = dict(zip(sites.tolist(), occ.tolist()))
+    occ_sorted = np.array([occ_map[int(x)] for x in sig_sorted], np.uint32)
+    ora = _oracle(pen_pos, pen_pam)
+    oix = ora.Index.load(idx_path)  # the reference-built index, read by the pinned oracle
+    traces = {}
+
+    def trace(g):
+        if g not in traces:
+            traces[g] = oix.trace(int(queries[g]))
+        return traces[g]
+
+    sel = [g for g in range(len(queries)) if len(trace(g)[0]) >= K["min_hits"]][:K["guides"]]
+    ent = knife_edge.entries(trace, sel)
+    qseqs = [synth.sig_to_seq(x) for x in queries.tolist()]
+
+    def one(i):
+        g, meth, t, _ = ent[i]
+        wd = os.path.join(tmp, f"k{i}")
+        os.makedirs(wd, exist_ok=True)
+        m, c, code = ref_module(idx_path, [qseqs[g] + "AGG"], meth, t, wd)
+        cnt, _ = ref_cli(idx_path, [qseqs[g]], CLI_NAME[meth], t, wd)
+        shutil.rmtree(wd)
+        return m[0], c[0], code[0], cnt[0]
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
+        res = list(pool.map(one, range(len(ent))))
+    differs = [knife_edge.exact_decision_differs(meth, t, *trace(g)[:2]) for g, meth, t, _ in ent]
+    arrays = {"sites": sig_sorted, "occ": occ_sorted, "queries": queries.astype(np.uint64),
+              "masks": synth.masks_from_strings(SLICE_CONFIGS[K["config"]]),
+              "guide": np.array([e[0] for e in ent], np.int32),
+              "method": np.array([knife_edge.METHODS[e[1]] for e in ent], np.int8),
+              "threshold": np.array([e[2] for e in ent], np.float64),
+              "aimed_hit": np.array([e[3] for e in ent], np.int32),
+              "mit": np.array([r[0] for r in res]), "cfd": np.array([r[1] for r in res]),
+              "code": np.array([r[2] for r in res], np.uint8), "count": np.array([r[3] for r in res], np.uint64),
+              "exact_differs": np.array(differs, bool)}
+    meta = dict(K, index_sha256=hashlib.sha256(open(idx_path, "rb").read()).hexdigest())
+    np.savez_compressed(os.path.join(HERE, "case_knife.npz"), meta=json.dumps(meta), **arrays)
+    print(f"knife: {len(ent)} (guide, method, threshold) entries on {len(sel)} guides, "
+          f"{sum(differs)} where exact sums would decide differently")
+
+
+C0_FULL = {"name": "c0_full", "seed": 1234, "n_sites": 1_000_000, "n_queries": 1000, "config": "slice-4-5",
+           "thresholds": {"mitAndCfd": [50.0, 75.0, 90.0], "mit": [75.0], "cfd": [75.0], "mitOrCfd": [75.0],
+                          "avgMitCfd": [75.0]}}
+
+
+def make_c0_full(tmp):
+    """Config 0 at its stated size: 1,000,000 i.i.d. sites (GC 41%), slice-4-5, 1,000 queries (500
+    copied from the sites, whose 0-4-substitution mutants join the site set, 500 random). Only
+    the outputs are stored: the sites are regenerated from the seed (synth.make_case) in the test."""
+    C = C0_FULL
+    sites, occ, queries = synth.make_case(C["seed"], C["n_sites"], C["n_queries"], repeat_frac=0.0,
+                                          planted_into_sites=True)
+    idx_path = os.path.join(tmp, "c0_full.issl")
+    ref_build_index(sites, occ, SLICE_CONFIGS[C["config"]], idx_path, tmp)
+    qseqs = [synth.sig_to_seq(x) for x in queries.tolist()]
+    guides = [x + "AGG" for x in qseqs]
+    arrays = {"queries": queries.astype(np.uint64)}
+    for meth, ts in C["thresholds"].items():
+        for t in ts:
+            m, c, codes = ref_module(idx_path, guides, meth, t, tmp)
+            cnt, distinct = ref_cli(idx_path, qseqs, CLI_NAME[meth], t, tmp)
+            key = f"{meth}_{t}"
+            arrays[f"mit_{key}"], arrays[f"cfd_{key}"], arrays[f"code_{key}"] = m, c, codes
+            arrays[f"count_{key}"] = cnt
+            arrays[f"distinct_{key}"] = np.array([distinct], np.uint64)
+    meta = dict(C, index_sha256=hashlib.sha256(open(idx_path, "rb").read()).hexdigest())
+    np.savez_compressed(os.path.join(HERE, "case_c0_full.npz"), meta=json.dumps(meta), **arrays)
+    print(f"c0_full: {C['n_sites']} sites, {len(queries)} queries, index {meta['index_sha256'][:12]}")
+
+
 def main():
     mit, pos, pam = parse_penalties()
     hdr, legacy = legacy_mit_pairs()
@@ -236,10 +342,17 @@ def main():
     with open(os.path.join(HERE, "penalties.json"), "w") as f:
         json.dump(payload, f, indent=0)
     print("penalties.json:", len(mit), "MIT pairs")
+    only = set(sys.argv[1:])  # optional: names of the fixtures to regenerate
     with tempfile.TemporaryDirectory() as tmp:
-        make_tiny(tmp)
+        if not only or "tiny" in only:
+            make_tiny(tmp)
         for c in CASES:
-            make_case(*c, tmp)
+            if not only or c[0] in only:
+                make_case(*c, tmp)
+        if not only or "knife" in only:
+            make_knife(tmp, pos, pam)
+        if not only or "c0_full" in only:
+            make_c0_full(tmp)
 
 
 if __name__ == "__main__":

@@ -145,6 +145,17 @@ def make_case(seed: int, n_sites: int, n_queries: int, repeat_frac: float = 0.05
     return sites.astype(U64), occ, queries[order]
 
 
+def reference_order(sigs: np.ndarray) -> np.ndarray:
+    """Sites in the order the reference's ISSLCreateIndex numbers them: ascending by their text
+    (it reads a sorted site list, ISSLCreateIndex.cpp:393-417). With A<C<G<T = 0<1<2<3 and the
+    first base most significant, numeric order of the reversed 2-bit groups is that order."""
+    s = np.ascontiguousarray(sigs, dtype=U64)
+    key = np.zeros(len(s), dtype=U64)
+    for j in range(20):
+        key |= ((s >> U64(2 * j)) & U64(3)) << U64(2 * (19 - j))
+    return s[np.argsort(key, kind="stable")]
+
+
 def sig_to_seq(sig: int, n: int = 20) -> str:
     return "".join("ACGT"[(int(sig) >> (2 * j)) & 3] for j in range(n))
 

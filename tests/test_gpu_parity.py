@@ -13,7 +13,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import CASE_NAMES, GOLDEN, load_case
+from conftest import CASE_NAMES, GOLDEN, c0_full_index, load_case
 
 pytestmark = pytest.mark.gpu
 
@@ -58,6 +58,24 @@ def test_golden_case(native, oracle_arrays, name):
     z, meta = load_case(name)
     with native.Index.from_arrays(*oracle_arrays(name)) as ix:
         check_golden(ix, z, meta)
+
+
+def test_config0_full_size(native, tmp_path):
+    """Config 0 at its stated size (1,000,000 sites, slice-4-5, 1,000 planted guides), built on the
+    GPU from the seeded sites: the index file equals the reference builder's byte for byte and
+    every method's results equal the reference's (module scores and codes, CLI counts and
+    distinct-site counts)."""
+    z, meta, sites, occ, masks = c0_full_index()
+    with native.Index.build(sites, occ, masks) as ix:
+        p = str(tmp_path / "c0.issl")
+        ix.save(p)
+        assert hashlib.sha256(open(p, "rb").read()).hexdigest() == meta["index_sha256"]
+        for meth, ts in meta["thresholds"].items():
+            for t in ts:
+                k = f"{meth}_{t}"
+                res = ix.score(z["queries"], meth, t)
+                assert_matches(res, z["mit_" + k], z["cfd_" + k], z["code_" + k].tobytes(), z["count_" + k],
+                               int(z["distinct_" + k][0]), tag=f"c0_full {k}")
 
 
 def test_tiny_genome_from_reference_file(native):
@@ -214,6 +232,49 @@ def test_module_filter_matches_reference(native):
     guides = [native.GuideResults(seq=s) for s in seqs]
     native.ISSLScoringModule(native.CracklingConfig(path, enabled=False)).run(guides)
     assert bytes(ord(g.passedOffTargetScore) for g in guides) == z["disabled_code"].tobytes()
+
+
+DROPIN = os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref", "module_dropin")
+
+
+def _run_dropin(index, seqs, flags, method, threshold, level, consensus_n, enabled, tmp):
+    """oracle/_ref/module_dropin: the reference's module driver, built with the reference's own
+    types and include/dropin/ISSLScoringModule.hpp over libissl_b200.so (oracle/Makefile)."""
+    gp, out = tmp / "guides.tsv", tmp / "out.tsv"
+    gp.write_text("".join(f"{s}\t{u}\t{c}\t{chr(b)}\n" for s, (u, c, b) in zip(seqs, flags)))
+    subprocess.run([DROPIN, index, str(gp), method, repr(threshold), level, str(consensus_n), str(enabled), str(out)],
+                   check=True, capture_output=True)
+    rows = [ln.split("\t") for ln in out.read_text().splitlines()]
+    return (np.array([float(r[1]) for r in rows]), np.array([float(r[2]) for r in rows]),
+            bytes(ord(r[3]) for r in rows))
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN), reason="oracle/_ref/module_dropin is built where the reference is")
+def test_dropin_module_with_reference_types(native, tmp_path):
+    """ISSLScoringModule as a Crackling++ pipeline would build it (src/CracklingPlusPlus.cpp:74-81):
+    the reference's cracklingConfig / guideResults, run() on a vector<guideResults>, every method
+    and threshold, every optimisation level of the processGuide filter, and the disabled module --
+    equal to the reference module's own outputs."""
+    from cracklingplusplus_gpu_b200.index import decode
+    z, meta = load_case("tiny")
+    index = os.path.join(GOLDEN, "tiny_genome.issl")
+    seqs = [decode(s) + "TGG" for s in z["queries"]]
+    plain = [(1, 0, ord("?"))] * len(seqs)
+    for meth in meta["methods"]:
+        for t in meta["thresholds"]:
+            k = f"{meth}_{t}"
+            m, c, codes = _run_dropin(index, seqs, plain, meth, t, "ultralow", 0, 1, tmp_path)
+            assert codes == z["code_" + k].tobytes(), k
+            np.testing.assert_allclose(m, z["mit_" + k], rtol=RTOL, atol=0, err_msg=k)
+            np.testing.assert_allclose(c, z["cfd_" + k], rtol=RTOL, atol=0, err_msg=k)
+    flags = [tuple(int(v) for v in f) for f in z["filter_flags"]]
+    for level in ["ultralow", "low", "medium", "high"]:
+        m, c, codes = _run_dropin(index, seqs, flags, "mitAndCfd", 75.0, level, 2, 1, tmp_path)
+        assert codes == z[f"filter_code_{level}"].tobytes(), level
+        np.testing.assert_allclose(m, z[f"filter_mit_{level}"], rtol=RTOL, atol=0, err_msg=level)
+        np.testing.assert_allclose(c, z[f"filter_cfd_{level}"], rtol=RTOL, atol=0, err_msg=level)
+    m, c, codes = _run_dropin(index, seqs, plain, "mitAndCfd", 75.0, "ultralow", 0, 0, tmp_path)
+    assert codes == z["disabled_code"].tobytes()
 
 
 def test_cli_output_matches_reference_format(native, tmp_path):

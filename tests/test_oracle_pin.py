@@ -16,7 +16,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import CASE_NAMES, GOLDEN, REPO, load_case
+from conftest import CASE_NAMES, GOLDEN, REPO, c0_full_index, load_case
 
 METHODS = {"mit": 0, "cfd": 1, "mitAndCfd": 2, "mitOrCfd": 3, "avgMitCfd": 4}
 
@@ -104,6 +104,61 @@ def test_early_exit_is_exercised(oracle):
     assert np.sum(tm_exit < tm_full) > 20 and np.sum(tc_exit < tc_full) > 20
 
 
+def _knife_entries(oracle):
+    z, meta = load_case("knife")
+    ix = oracle.Index.build(z["sites"], z["occ"], z["masks"])
+    return z, meta, ix
+
+
+def test_oracle_equals_reference_on_knife_edge_thresholds(oracle):
+    """Thresholds whose maximum_sum sits within a few ulps of a running sum: the oracle's
+    one-at-a-time sums reproduce the reference's scores, codes and counts bit for bit."""
+    z, meta, ix = _knife_entries(oracle)
+    with tempfile.TemporaryDirectory() as t:
+        p = os.path.join(t, "k.issl")
+        ix.write(p)
+        assert hashlib.sha256(open(p, "rb").read()).hexdigest() == meta["index_sha256"]
+    for i in range(len(z["guide"])):
+        g, m, thr = int(z["guide"][i]), int(z["method"][i]), float(z["threshold"][i])
+        tm, tc, cnt, _ = ix.score(z["queries"][g:g + 1], m, thr)
+        ms, cs, code = oracle.finalise(m, thr, tm, tc)
+        assert (ms[0], cs[0], code[0], int(cnt[0])) == (z["mit"][i], z["cfd"][i], z["code"][i], int(z["count"][i])), i
+
+
+def test_knife_edge_fixture_has_teeth(oracle):
+    """The knife-edge fixture exercises the reference's rounding: for many entries a decision
+    taken on exactly summed totals would differ, in every method, and the recorded flag agrees
+    with a recomputation from the oracle's trace of the guide."""
+    import knife_edge
+    z, meta, ix = _knife_entries(oracle)
+    names = list(knife_edge.METHODS)
+    assert int(z["exact_differs"].sum()) > 100
+    assert set(z["method"][z["exact_differs"]].tolist()) == set(range(5))
+    for i in range(0, len(z["guide"]), 7):
+        mt, ct, _ = ix.trace(int(z["queries"][int(z["guide"][i])]))
+        assert knife_edge.exact_decision_differs(names[int(z["method"][i])], float(z["threshold"][i]), mt, ct) == \
+            bool(z["exact_differs"][i])
+
+
+def test_oracle_equals_reference_config0_full(oracle):
+    z, meta, sites, occ, masks = c0_full_index()
+    ix = oracle.Index.build(sites, occ, masks)
+    with tempfile.TemporaryDirectory() as t:
+        p = os.path.join(t, "c0.issl")
+        ix.write(p)
+        assert hashlib.sha256(open(p, "rb").read()).hexdigest() == meta["index_sha256"]
+    for meth, ts in meta["thresholds"].items():
+        for t in ts:
+            k = f"{meth}_{t}"
+            tm, tc, cnt, dist = ix.score(z["queries"], METHODS[meth], t)
+            ms, cs, codes = oracle.finalise(METHODS[meth], t, tm, tc)
+            np.testing.assert_array_equal(ms, z["mit_" + k], err_msg=k)
+            np.testing.assert_array_equal(cs, z["cfd_" + k], err_msg=k)
+            assert codes == z["code_" + k].tobytes(), k
+            np.testing.assert_array_equal(cnt, z["count_" + k], err_msg=k)
+            assert dist == int(z["distinct_" + k][0]), k
+
+
 def test_slice_configs_match_fixture_masks():
     from cracklingplusplus_gpu_b200.slice_configs import slice_masks
     for name in CASE_NAMES:
@@ -112,7 +167,7 @@ def test_slice_configs_match_fixture_masks():
 
 
 REF_BIN = os.path.join(REPO, "oracle", "_ref")
-REF_SRC = "/root/reference"
+from refpath import REFERENCE as REF_SRC  # noqa: E402  (oracle/ is on the path, conftest.py)
 
 
 @pytest.mark.skipif(not (os.path.isdir(REF_SRC) and os.path.exists(os.path.join(REF_BIN, "ref_module_driver"))),
