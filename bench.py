@@ -73,7 +73,9 @@ def parse():
                     help="plain (default: the headline line), or any of batched, served (the slice-10-37 forms), "
                          "capacity (500M sites, slice-8-28), mapped (lists in host memory) and extract "
                          "(off-target extraction), comma-separated, one JSON line each")
-    ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the served-load run")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="length of the served-load run")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="plain line only (without the batched and served sub-objects on the slice-10-37 index)")
     ap.add_argument("--ref-cases", default=None, help="--impl reference --form gpu: cases to run (c0,c1)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="request arrivals per second (Poisson)")
     return ap.parse_args()
@@ -213,9 +215,16 @@ def cpu_baseline_port(ix, queries, method_id, threshold, target_s, gpu_res=None)
         parity = {"sample": n, "codes_equal": bytes(gpu_res.code[:n]) == codes,
                   "counts_equal": bool(np.array_equal(gpu_res.count[:n], cnt)),
                   "max_rel_err_mit": rel(gpu_res.mit[:n], ms), "max_rel_err_cfd": rel(gpu_res.cfd[:n], cs)}
+    one = queries[:max(16, n // cores)]  # the same oracle on one core, for about the same time
+    t0 = time.perf_counter()
+    oix.score(one, method_id, threshold, threads=1)
+    dt1 = time.perf_counter() - t0
     del oix, sigs, masks, sizes, lists
-    return {"value": n / dt, "unit": "guides/s", "cores": cores, "kind": "port",
-            "sample": f"first {n} of the {len(queries)} benchmark guides on the full index ({dt:.1f} s)"}, parity
+    return dict({"value": n / dt, "unit": "guides/s", "cores": cores, "kind": "port",
+                 "sample": f"first {n} of the {len(queries)} benchmark guides on the full index ({dt:.1f} s)",
+                 "single_core": {"value": len(one) / dt1, "unit": "guides/s", "cores": 1,
+                                 "sample": f"the first {len(one)} of those guides ({dt1:.1f} s)"}},
+                **host_info()), parity
 
 
 def run_ours(args):
@@ -353,48 +362,98 @@ def run_ours(args):
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     ix.close()
+    if rank == 0 and world == 1 and not args.no_forms:
+        # the batched and served forms on their own index (300M sites, slice-10-37), after the
+        # plain index is gone: sub-objects of the same line
+        line.update(forms_on_slice10_index(args))
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
+def host_info():
+    """CPU model, host RAM and hardware threads of this machine (for the CPU baseline's record)."""
+    model, ram = None, None
+    try:
+        model = next(ln.split(":", 1)[1].strip() for ln in open("/proc/cpuinfo") if ln.startswith("model name"))
+    except (OSError, StopIteration):
+        pass
+    try:
+        kb = next(int(ln.split()[1]) for ln in open("/proc/meminfo") if ln.startswith("MemTotal"))
+        ram = round(kb / 1048576, 1)
+    except (OSError, StopIteration):
+        pass
+    return {"cpu_model": model, "host_ram_gib": ram, "host_threads": os.cpu_count()}
+
+
+def slice_masks_of(name):
+    """Slice masks from the pure-data slice_configs module, loaded by path (the reference arm never
+    imports the library's package, which would load libissl_b200.so)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "_slice_configs", os.path.join(REPO, "cracklingplusplus_gpu_b200", "slice_configs.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.slice_masks(name)
+
+
+def seq_of(sig) -> str:
+    """2-bit packed 20-mer (base j at bits 2j, A=0 C=1 G=2 T=3) -> text."""
+    return "".join("ACGT"[(int(sig) >> (2 * j)) & 3] for j in range(20))
+
+
+def run_reference_cli(binary, idx, guides, cores, workdir):
+    """One run of the reference's ISSLScoreOfftargets on `guides`; returns its 'ISSL scoring time'."""
+    qf = os.path.join(workdir, "queries.txt")
+    with open(qf, "w") as f:
+        f.write("".join(seq_of(s) + "\n" for s in guides))
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    r = subprocess.run([binary, idx, qf, "4", str(WORKLOAD["threshold"]), WORKLOAD["method"], "out.txt"],
+                       cwd=workdir, env=env, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference exited {r.returncode}: {r.stderr.strip()[-200:]}")
+    return float(re.search(r"ISSL scoring time: ([0-9.eE+-]+) seconds", r.stdout).group(1))
+
+
 def run_reference(args):
-    """The reference's own CPU scorer on the same workload, all host cores."""
+    """The reference's own CPU scorer on the same workload: all host cores, plus one core.
+
+    The index is generated and written by the oracle's host restatement of the library's seeded
+    generator (oracle/synth_oracle.c) with the reference builder's layout: no code of the library
+    runs in this arm."""
     world, rank, local = dist_env()
     if rank != 0:
         return
     binary = os.path.join(REPO, "oracle", "_ref", "ISSLScoreOfftargets")
-    spec_sites = args.sites or WORKLOAD["n_sites"]
     if not os.path.exists(binary):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ISSLScoreOfftargets was not built "
                           "(needs the reference sources at build time)"}))
         return
-    import cracklingplusplus_gpu_b200 as pkg
-    from cracklingplusplus_gpu_b200 import build
-    from cracklingplusplus_gpu_b200.index import decode
-    build.build()
-    spec, n_sites, nq = spec_for(args, 1)
-    ix, q = pkg.Index.synth(spec, device=local)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle")], check=True)
+    import pyoracle
+    n_sites = args.sites or WORKLOAD["n_sites"]
+    nq = args.queries or WORKLOAD["n_queries"]
     cores = int(os.environ.get("ISSL_REF_THREADS", "0")) or os.cpu_count() or 1  # default: every host core
     workdir = tempfile.mkdtemp(dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
     try:
+        t0 = time.time()
+        sites, occ, q = pyoracle.synth(WORKLOAD["seed"], n_sites, nq, repeat_frac=WORKLOAD["repeat_frac"],
+                                       n_repeat_seeds=WORKLOAD["repeat_seeds"], repeat_lambda=WORKLOAD["repeat_lambda"],
+                                       copied_frac=0.5)
         idx = os.path.join(workdir, "index.issl")
-        ix.save(idx)
-        ix.close()
+        pyoracle.write_built(idx, sites, occ, np.array(slice_masks_of(WORKLOAD["slice_config"]), np.uint64))
+        del sites, occ
+        gen_s = time.time() - t0
         # bounded sample: K steps of `per_step` guides scored in one invocation of the reference
-        per_step = max(64, int(os.environ.get("ISSL_REF_GUIDES_PER_STEP", "0")) or (200 if spec_sites >= 10**8 else 1000))
-        total = per_step * args.steps
-        sample = q[:total]
-        qf = os.path.join(workdir, "queries.txt")
-        with open(qf, "w") as f:
-            f.write("".join(decode(s) + "\n" for s in sample))
-        env = dict(os.environ, OMP_NUM_THREADS=str(cores))
-        r = subprocess.run([binary, idx, qf, "4", str(WORKLOAD["threshold"]), WORKLOAD["method"], "out.txt"],
-                           cwd=workdir, env=env, capture_output=True, text=True)
-        if r.returncode != 0:
-            print(json.dumps({"impl": "reference", "unavailable": f"reference exited {r.returncode}: "
-                              f"{r.stderr.strip()[-200:]}"}))
-            return
-        t = float(re.search(r"ISSL scoring time: ([0-9.eE+-]+) seconds", r.stdout).group(1))
+        per_step = max(64, int(os.environ.get("ISSL_REF_GUIDES_PER_STEP", "0")) or (200 if n_sites >= 10**8 else 1000))
+        sample = q[:per_step * args.steps]
+        t = run_reference_cli(binary, idx, sample, cores, workdir)
+        # the same reference on one core, on a sample sized for about the same time
+        one = q[:max(16, len(sample) // cores)]
+        t1 = run_reference_cli(binary, idx, one, 1, workdir)
+    except RuntimeError as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+        return
     finally:
         shutil.rmtree(workdir, ignore_errors=True)
     value = len(sample) / t
@@ -403,9 +462,14 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 integer scan, f64 sums", "data": "synthetic",
         "config": dict(WORKLOAD, n_sites=n_sites, n_queries=nq, parallelism="host cores"),
-        "cpu_baseline": {"value": value, "unit": "guides/s", "cores": cores, "kind": "reference",
-                         "sample": f"{len(sample)} guides ({per_step} per step) of the benchmark set on the full "
-                                   f"index; the reference's own 'ISSL scoring time'"},
+        "cpu_baseline": dict({"value": value, "unit": "guides/s", "cores": cores, "kind": "reference",
+                              "sample": f"{len(sample)} guides ({per_step} per step) of the benchmark set on the full "
+                                        f"index; the reference's own 'ISSL scoring time'",
+                              "single_core": {"value": len(one) / t1, "unit": "guides/s", "cores": 1,
+                                              "sample": f"the first {len(one)} of those guides, OMP_NUM_THREADS=1"},
+                              "build": "g++ -O3 -march=x86-64-v3 -fopenmp (oracle/Makefile)",
+                              "index_from": "oracle/synth_oracle.c (host restatement of the seeded generator), "
+                                            f"{gen_s:.0f} s"}, **host_info()),
         "e2e": {"value": value, "unit": "guides/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -533,7 +597,71 @@ SERVED = {"workload": "issl-score served: 300M-site slice-10-37 index, Poisson a
 CAPACITY = {"workload": "issl-score capacity: 500M-site slice-8-28 index, 5M guides (90% random, 10% repeat-derived), "
                         "MIT+CFD 'and', threshold 75, max 4 mismatches",
             "n_sites": 500_000_000, "slice_config": "slice-8-28", "n_queries": 5_000_000, "copied_frac": 0.0,
-            "repeat_query_frac": 0.1, "seed": 1237, "method": "and", "threshold": 75.0, "max_dist": 4}
+            "repeat_query_frac": 0.1, "seed": 1237, "method": "and", "threshold": 75.0, "max_dist": 4,
+            "parity_guides": 50_000}
+
+
+def reference_parity_streamed(ix, q, res, method_word, thr, n):
+    """The reference's own ISSLScoreOfftargets (the build without FMA contraction) scores the first n
+    guides on the same index, which is streamed to it through a named pipe: at 500M sites x 28 slices
+    the reference's in-memory copy alone takes 116 GB of host memory, so the index never exists as a
+    file. Off-target counts must be equal; the reference prints scores with six decimals, so scores
+    must agree to that and the accept codes are compared wherever the printed scores decide them."""
+    binary = os.path.join(REPO, "oracle", "_ref", "ISSLScoreOfftargets_exact")
+    if not os.path.exists(binary):
+        return {"skipped": "oracle/_ref/ISSLScoreOfftargets_exact was not built (needs the reference sources)"}
+    workdir = tempfile.mkdtemp(dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        fifo = os.path.join(workdir, "index.issl")
+        os.mkfifo(fifo)
+        sample = q[:n]
+        qf = os.path.join(workdir, "queries.txt")
+        with open(qf, "w") as f:
+            f.write("".join(seq_of(x) + "\n" for x in sample))
+        proc = subprocess.Popen([binary, fifo, qf, "4", repr(thr), method_word, "cap_out.txt"], cwd=workdir,
+                                stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+        err = []
+
+        def writer():
+            try:
+                ix.save(fifo)
+            except Exception as e:  # the reader went away: reported below
+                err.append(str(e))
+
+        t0 = time.time()
+        w = threading.Thread(target=writer, daemon=True)
+        w.start()
+        out, errtxt = proc.communicate()
+        if w.is_alive():  # the reference exited without reading: release the writer
+            with open(fifo, "rb") as f:
+                while f.read(1 << 20):
+                    pass
+        w.join()
+        wall = time.time() - t0
+        if proc.returncode != 0 or err:
+            return {"skipped": f"reference exited {proc.returncode}: {errtxt.strip()[-200:]} {err}"}
+        t_score = float(re.search(r"ISSL scoring time: ([0-9.eE+-]+) seconds", out).group(1))
+        rows = [ln.split("\t") for ln in out.splitlines() if ln.count("\t") == 2]
+        files = [p for p in os.listdir(workdir) if p.endswith("cap_out.txt")]
+        counts = [int(ln.rstrip("\n").split("\t")[3]) for ln in open(os.path.join(workdir, files[0]))
+                  if not ln.startswith("#")]
+    finally:
+        shutil.rmtree(workdir, ignore_errors=True)
+    rm = np.array([float(r[1]) for r in rows])
+    rc = np.array([float(r[2]) for r in rows])
+    ours_code = np.frombuffer(res.code[:n], np.uint8)
+    # 'and': rejected when both scores are below the threshold; a printed score within its rounding
+    # (5e-7) of the threshold does not decide
+    decided = (np.abs(rm - thr) > 1e-6) & (np.abs(rc - thr) > 1e-6)
+    ref_code = np.where((rm < thr) & (rc < thr), ord("0"), ord("1")).astype(np.uint8)
+    return {
+        "sample": len(rows), "reference": "oracle/_ref/ISSLScoreOfftargets_exact, index streamed through a named pipe",
+        "counts_equal": bool(np.array_equal(np.array(counts, np.uint64), res.count[:n])),
+        "codes_equal": bool(np.array_equal(ours_code[decided], ref_code[decided])),
+        "codes_undecided_by_printed_scores": int((~decided).sum()),
+        "max_abs_score_diff_vs_printed": float(max(np.max(np.abs(rm - res.mit[:n])), np.max(np.abs(rc - res.cfd[:n])))),
+        "cpu_guides_per_s": len(rows) / t_score, "cpu_cores": os.cpu_count(), "wall_s": wall,
+    }
 
 
 def bench_capacity(args, pkg):
@@ -591,16 +719,9 @@ def bench_capacity(args, pkg):
     res = pkg.ScoreResult(d_mit.cpu().numpy(), d_cfd.cpu().numpy(), bytes(d_code.cpu().numpy()),
                           d_cnt.cpu().numpy().view(np.uint64), None)
     parity = None
-    import psutil
-    need = n_sites * info.n_slices * 8 * 1.3
-    if not args.no_cpu and psutil.virtual_memory().available > need:
-        ix.trim()  # the export stages each slice's lists through device memory
-        cpu, parity = cpu_baseline_port(ix, q, meth, thr, min(args.cpu_seconds, 20.0), res)
-        parity["cpu_guides_per_s"] = cpu["value"]
-        parity["cpu_cores"] = cpu["cores"]
-    else:
-        parity = {"skipped": f"host memory {psutil.virtual_memory().available / 1e9:.0f} GB < {need / 1e9:.0f} GB "
-                             "for the exported index"}
+    if not args.no_cpu:
+        ix.trim()  # the index file is written from device memory through staging buffers
+        parity = reference_parity_streamed(ix, q, res, CAPACITY["method"], thr, CAPACITY["parity_guides"])
     ix.close()
     return {
         "metric": "guides/sec, capacity run (500M-site slice-8-28 index, 5M guides, 1 B200)",
@@ -813,6 +934,16 @@ def run_forms(args, forms):
     forms = [f for f in forms if f not in ("capacity", "extract", "mapped")]
     if not forms:
         return
+    ix, q, base = slice10_index(args, pkg, local)
+    if "batched" in forms:
+        print(json.dumps(bench_batched(args, pkg, ix, q, base)), flush=True)
+        ix.trim()  # the plain calls' workspace is not needed by the server
+    if "served" in forms:
+        print(json.dumps(bench_served(args, pkg, ix, q, base)), flush=True)
+    ix.close()
+
+
+def slice10_index(args, pkg, local):
     n_sites = args.sites or FORMS["n_sites"]
     pool = args.queries or FORMS["pool"]
     spec = pkg.SynthSpec(seed=FORMS["seed"], n_sites=n_sites, slice_config=FORMS["slice_config"], n_queries=pool,
@@ -824,12 +955,19 @@ def run_forms(args, forms):
     base = {"n_sites": n_sites, "slice_config": FORMS["slice_config"], "seed": FORMS["seed"],
             "repeat_query_frac": FORMS["repeat_query_frac"], "generation_s": gen_s}
     log(f"index: {n_sites} sites, {FORMS['slice_config']}, {pool} pool guides, generated in {gen_s:.1f} s")
-    if "batched" in forms:
-        print(json.dumps(bench_batched(args, pkg, ix, q, base)), flush=True)
-        ix.trim()  # the plain calls' workspace is not needed by the server
-    if "served" in forms:
-        print(json.dumps(bench_served(args, pkg, ix, q, base)), flush=True)
+    return ix, q, base
+
+
+def forms_on_slice10_index(args):
+    """{"batched": ..., "served": ...} on the slice-10-37 index, for the headline line."""
+    import torch
+    import cracklingplusplus_gpu_b200 as pkg
+    ix, q, base = slice10_index(args, pkg, torch.cuda.current_device())
+    out = {"batched": bench_batched(args, pkg, ix, q, base)}
+    ix.trim()  # the plain calls' workspace is not needed by the server
+    out["served"] = bench_served(args, pkg, ix, q, base)
     ix.close()
+    return out
 
 
 def log(msg):
@@ -973,6 +1111,7 @@ def bench_served(args, pkg, ix, q, base):
     next_t = start
     n_req = offered = 0
     sample_reqs = []
+    arrivals = []  # (arrival time, request): the same request set for the plain form below
     while True:
         next_t += rng.exponential(1.0 / rate)
         if next_t - start > seconds:
@@ -984,6 +1123,7 @@ def bench_served(args, pkg, ix, q, base):
         t = srv.submit(*req)
         n_req += 1
         offered += len(req[0])
+        arrivals.append((time.perf_counter() - start, req))
         tickets.put((t, len(req[0]), req if len(sample_reqs) < 40 and n_req % 25 == 0 else None))
     for _ in cols:
         tickets.put(None)
@@ -1003,6 +1143,23 @@ def bench_served(args, pkg, ix, q, base):
         alone = ix.score(req[0], req[1], req[2], max_dist=req[3], distinct=False)
         mixed_ok &= alone.code == res.code and np.array_equal(alone.mit, res.mit) and np.array_equal(alone.cfd, res.cfd)
         checked += 1
+    # the plain form on the same request set: one query file at a time through issl_score_sigs (host
+    # buffers, no batching, no overlap); latency under the same arrivals follows from its service
+    # times with a first-come-first-served queue
+    service = []
+    t_plain = time.perf_counter()
+    for _, req in arrivals:
+        t1 = time.perf_counter()
+        ix.score(req[0], req[1], req[2], max_dist=req[3], distinct=False)
+        service.append(time.perf_counter() - t1)
+    plain_wall = time.perf_counter() - t_plain
+    done, plain_lat = 0.0, []
+    for (a, _), sv in zip(arrivals, service):
+        done = max(done, a) + sv
+        plain_lat.append((done - a) * 1e3)
+    plain_lat = np.array(plain_lat)
+    plain_k = np.array([len(r[0]) for _, r in arrivals])
+    plain_one_k = plain_lat[(plain_k >= 500) & (plain_k <= 2000)]
     return {
         "metric": "served latency p99 (ms), MIT/CFD <=4 mm, 300M-site slice-10-37 index",
         "value": float(np.percentile(lat, 99)), "unit": "ms", "higher_is_better": False, "n_gpus": 1,
@@ -1014,6 +1171,13 @@ def bench_served(args, pkg, ix, q, base):
         "batches": int(st.batches), "mean_batch_guides": st.mean_batch_guides, "peak_in_flight": int(st.peak_in_flight),
         "slots": int(st.slots), "slot_budget_bytes": int(st.slot_budget_bytes), "peak_batch_bytes": int(st.peak_batch_bytes),
         "mixed_equals_alone": {"checked": checked, "equal": bool(mixed_ok)},
+        "plain_same_requests": {
+            "guides_per_s": float(plain_k.sum() / plain_wall), "service_p50_ms": float(np.percentile(service, 50) * 1e3),
+            "service_p99_ms": float(np.percentile(service, 99) * 1e3),
+            "queued_p50_ms": float(np.percentile(plain_lat, 50)), "queued_p99_ms": float(np.percentile(plain_lat, 99)),
+            "queued_p99_ms_1k_guide_requests": float(np.percentile(plain_one_k, 99)) if len(plain_one_k) else None,
+            "note": "one issl_score_sigs call per request, back to back; queued latencies replay the served run's "
+                    "arrival times through a single first-come-first-served queue of these service times"},
         "data": "synthetic (seeded, generated on device)", "config": dict(SERVED, **base),
     }
 

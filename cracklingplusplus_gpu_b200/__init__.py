@@ -9,7 +9,8 @@ Python mirrors of the reference's interfaces:
   * ``Index``              -- a resident index: ``Index.open(path)`` replaces the per-call .issl read
                               of lib/ISSLScoringModule.cpp:72-150; ``score()`` is the scoring loop
   * ``ISSLScoringModule``  -- same constructor/run() contract as include/ISSLScoringModule.hpp:15-29
-                              (drives the C++ drop-in class through ``issl_module_run``)
+                              (through ``issl_module_run``, the C entry point behind the
+                              header-only C++ class of include/issl_b200_module.hpp)
   * ``OT_METHODS`` / ``CLI_METHODS`` -- otScoreMethod numbering and the CLI's method words
 
 Beyond the reference: ``Batch`` scores many guide sets (each with its own method, threshold and

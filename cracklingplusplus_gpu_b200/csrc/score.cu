@@ -509,10 +509,23 @@ struct ScanShared {  // per-block slice tables
     uint8_t wpb[kMaxSlices], rw[kMaxSlices];
 };
 
-struct ScanCtx {  // per-warp state of the candidate slab
-    uint32_t cpos, cend;
-    bool full;
+// A warp's pending candidate records: lane i holds the i-th, and every 32 of them are written with
+// one reservation and one coalesced store.
+struct ScanCtx {
+    uint32_t x, y, z;  // this lane's pending record
+    uint32_t n;        // pending records in the warp (the same in every lane)
 };
+
+__device__ __forceinline__ void flush_cands(const ScanArgs& a, ScanCtx& cx, int lane) {
+    if (!cx.n) return;
+    unsigned long long b = 0;
+    if (lane == 0) b = atomicAdd(&a.counters->cand_reserved, static_cast<unsigned long long>(cx.n));
+    b = __shfl_sync(0xffffffffu, b, 0);
+    // 64-bit reservations: a wave may ask for more slots than the buffer holds (the host then grows
+    // it, or splits the guides, and reruns); slots past the capacity are counted, never written
+    if (b + cx.n <= a.cand_cap && static_cast<uint32_t>(lane) < cx.n) a.cands[b + lane] = make_uint4(cx.x, cx.y, cx.z, 0u);
+    cx.n = 0;
+}
 
 // Compares every guide of the unit with the lane's block (RW residual positions per entry).
 template <int RW>
@@ -520,15 +533,16 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
                                           const StageMeta& m, uint32_t wpb, int lane, int max_dist, ScanCtx& cx) {
     constexpr int NW = 2 * RW;
     constexpr int NV = (NW + 3) / 4;
-    const unsigned lt = (1u << lane) - 1u;
-    // this lane's block and the entries of it that belong to the unit
+    // this lane's block and the entries of it that belong to the unit (unsigned arithmetic: list
+    // positions reach 2^32 - 1; the unit starts in block b0 and ends after this lane's block start)
     uint32_t d[NW];
     uint32_t valid = 0;
     const uint32_t bl = m.b0 + lane;
     if (static_cast<uint32_t>(lane) < m.nb) {
-        const int lo = max(static_cast<int>(m.p0) - static_cast<int>(32 * bl), 0);
-        const int hi = min(static_cast<int>(m.p0 + m.len) - static_cast<int>(32 * bl), 32);
-        valid = (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
+        const uint32_t base = 32u * bl, end = m.p0 + m.len;
+        const uint32_t lo = m.p0 > base ? m.p0 - base : 0u;
+        const uint32_t hi = end - base >= 32u ? 32u : end - base;
+        valid = (hi >= 32u ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
     }
     // odd block stride: the 32 lanes read 32 different banks. Words of lanes past the unit are
     // stale but masked by `valid`.
@@ -563,39 +577,41 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
             if (2 * v < RW) mm[2 * v] = (d[4 * v] ^ w.x) | (d[4 * v + 1] ^ w.y);
             if (2 * v + 1 < RW) mm[2 * v + 1] = (d[4 * v + 2] ^ w.z) | (d[4 * v + 3] ^ w.w);
         }
-        uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), max_dist) & valid;
-        // candidates are rare: one per lane per round, written to the warp's slab as
-        // (guide | slice << 26, list position, residual mismatch mask); k_cand_own applies the
-        // ownership rule to the mask
-        for (unsigned hm = __ballot_sync(0xffffffffu, cbits != 0); hm; hm = __ballot_sync(0xffffffffu, cbits != 0)) {
-            const uint32_t nh = __popc(hm);
-            if (cx.cpos + nh > cx.cend) {
-                // retire the rest of the slab, reserve a new one
-                for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
-                    if (i < a.cand_cap) a.cands[i] = make_uint4(kDeadCand, 0, 0, 0);
-                // 64-bit reservations: a wave may ask for more than 2^32 slots (the host then splits
-                // the guides); a slab past the capacity is never written
-                uint32_t base = 0, full = 0;
-                if (lane == 0) {
-                    const unsigned long long b = atomicAdd(&a.counters->cand_reserved, static_cast<unsigned long long>(kCandSlab));
-                    full = b + kCandSlab > a.cand_cap;
-                    base = full ? a.cand_cap : static_cast<uint32_t>(b);
+        const uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), max_dist) & valid;
+        // Candidates are rare. The warp takes them one at a time: lane p tests residual position p
+        // of the candidate's entry against the guide, straight from the staged block, and one
+        // ballot gives the candidate's residual mismatch mask (k_cand_own applies the ownership
+        // rule to it). Records are (guide | slice << 26, list position, mask).
+        unsigned hm = __ballot_sync(0xffffffffu, cbits != 0);
+        if (hm) {
+            uint32_t q0 = 0, q1 = 0;  // the guide's two bits at residual position `lane`, spread
+            if (lane < RW) {
+                const uint32_t rq = static_cast<uint32_t>(g >> 32);
+                q0 = 0u - ((rq >> (2 * lane)) & 1u);
+                q1 = 0u - ((rq >> (2 * lane + 1)) & 1u);
+            }
+            const uint32_t gx = static_cast<uint32_t>(g) | (m.s << kGuideBits);
+            do {
+                const int src = __ffs(hm) - 1;
+                hm &= hm - 1;
+                uint32_t cb = __shfl_sync(0xffffffffu, cbits, src);
+                uint32_t mw = 0;  // bit e: entry e of block src mismatches at position `lane`
+                if (lane < RW) {
+                    const uint32_t* sb = rb + m.delta + src * wpb;
+                    mw = (sb[2 * lane] ^ q0) | (sb[2 * lane + 1] ^ q1);
                 }
-                cx.cpos = __shfl_sync(0xffffffffu, base, 0);
-                cx.cend = cx.cpos + kCandSlab;
-                cx.full = __shfl_sync(0xffffffffu, full, 0) != 0;
-            }
-            if (cbits) {
-                const int e = __ffs(cbits) - 1;
-                cbits &= cbits - 1;
-                uint32_t rm = 0;  // bit p: residual position p of entry e mismatches the guide
-#pragma unroll
-                for (int p = 0; p < RW; p++) rm |= ((mm[p] >> e) & 1u) << p;
-                if (!cx.full)
-                    a.cands[cx.cpos + __popc(hm & lt)] =
-                        make_uint4(static_cast<uint32_t>(g) | (m.s << kGuideBits), 32u * bl + e, rm, 0u);
-            }
-            cx.cpos += nh;
+                do {
+                    const int e = __ffs(cb) - 1;
+                    cb &= cb - 1;
+                    const uint32_t rmask = __ballot_sync(0xffffffffu, (mw >> e) & 1u);
+                    if (static_cast<uint32_t>(lane) == cx.n) {
+                        cx.x = gx;
+                        cx.y = 32u * (m.b0 + static_cast<uint32_t>(src)) + static_cast<uint32_t>(e);
+                        cx.z = rmask;
+                    }
+                    if (++cx.n == 32u) flush_cands(a, cx, lane);
+                } while (cb);
+            } while (hm);
         }
     }
 }
@@ -696,7 +712,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
         issued++;
     };
 
-    ScanCtx cx{0u, 0u, false};
+    ScanCtx cx{0u, 0u, 0u, 0u};
     for (uint32_t i = 0; i < NS; i++) try_issue();
     __syncwarp();
 
@@ -738,8 +754,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
         if (lane == 0) atomicOr(&a.counters->overflow, 4u);
         for (uint32_t u = t; u < issued; u++) mbar_wait_bounded(&bar[u % NS], (u / NS) & 1u, kWaitCycles);
     }
-    for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
-        if (i < a.cand_cap) a.cands[i] = make_uint4(kDeadCand, 0, 0, 0);
+    flush_cands(a, cx, lane);
 }
 
 __global__ void k_cands_finalize(Counters* c, uint32_t cand_cap) {

@@ -82,6 +82,18 @@ int ora_score(const ora_index* idx, const uint64_t* query_sigs, uint64_t n_queri
 uint64_t ora_trace(const ora_index* idx, uint64_t query_sig, int max_dist, double* mit_terms,
                    double* cfd_terms, uint32_t* occ, uint64_t cap);
 
+/* Synthetic workloads (synth_oracle.c): the library's seeded generator restated for the host.
+ * sites[n_sites], occ[n_sites], queries[n_queries] receive the workload issl_synth generates for
+ * the same spec. Returns 0, -1 (allocation) or -2 (not enough distinct sites). */
+int ora_synth(uint64_t seed, uint64_t n_sites, double repeat_frac, uint64_t n_repeat_seeds,
+              double repeat_lambda, uint64_t n_queries, double copied_frac, double repeat_query_frac,
+              int planted_into_sites, uint64_t* sites, uint32_t* occ, uint64_t* queries);
+
+/* Writes the .issl file of sites + occurrences bucketed by the slice masks (ISSLCreateIndex.cpp
+ * :428-484 layout), one slice at a time (OpenMP). 0 on success. */
+int ora_write_built(const char* path, const uint64_t* sigs, const uint32_t* occ, uint64_t n_sites,
+                    const uint64_t* slice_masks, uint64_t n_slices);
+
 /* Per-guide finalisation, lib/ISSLScoringModule.cpp:404-459: scores and the accept code
  * ('1' accepted / '0' rejected). For mit (cfd) the unused score is -1. */
 void ora_finalise(int method, double threshold, double tot_mit, double tot_cfd, double* mit_score,

@@ -59,6 +59,10 @@ def lib():
                                    P(C.c_double), C.c_char_p]
         L.ora_bruteforce.argtypes = [P(C.c_uint64), P(C.c_uint32), C.c_uint64, P(C.c_uint64), C.c_uint64,
                                      C.c_int, C.c_int, P(C.c_double), P(C.c_double), P(C.c_uint64)]
+        L.ora_synth.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_double, C.c_uint64, C.c_double,
+                                C.c_double, C.c_int, P(C.c_uint64), P(C.c_uint32), P(C.c_uint64)]
+        L.ora_write_built.argtypes = [C.c_char_p, P(C.c_uint64), P(C.c_uint32), C.c_uint64, P(C.c_uint64),
+                                      C.c_uint64]
         L.ora_trace.restype = C.c_uint64
         L.ora_trace.argtypes = [C.POINTER(OraIndex), C.c_uint64, C.c_int, P(C.c_double), P(C.c_double),
                                 P(C.c_uint32), C.c_uint64]
@@ -175,6 +179,33 @@ class Index:
             self.free()
         except Exception:
             pass
+
+
+def synth(seed: int, n_sites: int, n_queries: int, repeat_frac: float = 0.05, n_repeat_seeds: int = 10000,
+          repeat_lambda: float = 2.0, copied_frac: float = 0.5, repeat_query_frac: float = 0.0,
+          planted_into_sites: bool = False, threads: int = 0):
+    """The library's seeded synthetic workload (issl_synth's spec), generated on the host:
+    (sites uint64[n_sites], occ uint32[n_sites], queries uint64[n_queries])."""
+    sites = np.zeros(n_sites, np.uint64)
+    occ = np.zeros(n_sites, np.uint32)
+    q = np.zeros(max(n_queries, 1), np.uint64)
+    rc = lib().ora_synth(seed, n_sites, repeat_frac, n_repeat_seeds, repeat_lambda, n_queries, copied_frac,
+                         repeat_query_frac, int(planted_into_sites), _p(sites, C.c_uint64), _p(occ, C.c_uint32),
+                         _p(q, C.c_uint64))
+    if rc != 0:
+        raise RuntimeError(f"oracle synth failed (rc={rc})")
+    return sites, occ, q[:n_queries]
+
+
+def write_built(path: str, sigs, occ, masks) -> None:
+    """Writes the .issl file of the sites bucketed by the slice masks (reference builder layout)."""
+    sigs = np.ascontiguousarray(sigs, np.uint64)
+    occ = np.ascontiguousarray(occ, np.uint32)
+    masks = np.ascontiguousarray(masks, np.uint64)
+    rc = lib().ora_write_built(path.encode(), _p(sigs, C.c_uint64), _p(occ, C.c_uint32), len(sigs),
+                               _p(masks, C.c_uint64), len(masks))
+    if rc != 0:
+        raise RuntimeError(f"oracle: cannot write {path}")
 
 
 def finalise(method: int, threshold: float, tot_mit, tot_cfd):

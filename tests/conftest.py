@@ -68,3 +68,15 @@ def c0_full_index():
     occ_sorted = np.array([occ_of[int(s)] for s in order.tolist()], np.uint32)
     np.testing.assert_array_equal(queries, z["queries"])
     return z, meta, order, occ_sorted, np.array(slice_masks(meta["config"]), np.uint64)
+
+
+def extract_fixture(root):
+    """Writes the extraction fixture's input files under `root`; returns (input paths as the
+    reference was given them, the reference's output bytes, meta)."""
+    z, meta = load_case("extract")
+    for i, rel in enumerate(meta["inputs"]):
+        p = os.path.join(root, rel)
+        os.makedirs(os.path.dirname(p), exist_ok=True)
+        with open(p, "wb") as f:
+            f.write(z[f"input_{i}"].tobytes())
+    return [os.path.join(root, a) for a in meta["args"]], z["output"].tobytes(), meta

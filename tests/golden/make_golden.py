@@ -18,6 +18,8 @@ Outputs
                      (guide, method, threshold) per entry, scored by the same two binaries
   case_c0_full.npz   config 0 at its stated size (1M sites, slice-4-5, 1,000 guides): outputs
                      only, the sites are regenerated from the seed
+  case_extract.npz   the reference's ExtractOfftargets on a small genome collection: the input
+                     files and its output file
 
 python tests/golden/make_golden.py [names...] regenerates only the named fixtures.
 """
@@ -325,6 +327,62 @@ def make_c0_full(tmp):
     print(f"c0_full: {C['n_sites']} sites, {len(queries)} queries, index {meta['index_sha256'][:12]}")
 
 
+def extract_inputs(seed=21):
+    """A small genome collection for the extractor, every input form the reference reads: a FASTA
+    file with CRLF lines, lower-case stretches, N runs and copied stretches (duplicate sites); a
+    plain file of one sequence per line; a directory holding a FASTA file with an empty record line
+    and a plain file without a final newline. Returns {relative path: bytes}."""
+    st = synth.Stream(seed, 31)
+
+    def genome(n):
+        b = bytearray(np.frombuffer(b"ACGT", np.uint8)[synth.gc41_bases(st.uniform(n)).astype(np.int64)].tobytes())
+        for _ in range(n // 2000):  # copied stretches
+            a, c = (int(x) for x in st.below(2, n - 200))
+            b[c:c + 150] = b[a:a + 150]
+        for _ in range(n // 5000):  # N runs
+            a, k = int(st.below(1, n - 50)[0]), 1 + int(st.below(1, 40)[0])
+            b[a:a + k] = b"N" * k
+        for _ in range(n // 8000):  # soft-masked (lower-case) stretches
+            a = int(st.below(1, n - 300)[0])
+            b[a:a + 300] = bytes(b[a:a + 300]).lower()
+        return bytes(b[:n])
+
+    fa = b""
+    for r in range(3):
+        g = genome(30000 + 7000 * r)
+        fa += b">chr%d synthetic\r\n" % r + b"".join(g[i:i + 60] + b"\r\n" for i in range(0, len(g), 60))
+    lines = b"\n".join(genome(400 + 50 * i) for i in range(20)) + b"\n"
+    a_fa = b">x\n" + genome(5000) + b"\n>y\n\n" + genome(3000) + b"\n"
+    b_txt = genome(2500)
+    return {"g.fa": fa, "lines.txt": lines, "more/a.fa": a_fa, "more/b.txt": b_txt}
+
+
+def make_extract(tmp):
+    """The reference's own ExtractOfftargets (built with read-only std::regex / <cctype> stand-ins
+    for its two Boost headers, oracle/Makefile) on extract_inputs(): its output file, byte for byte."""
+    inputs = extract_inputs()
+    root = os.path.join(tmp, "extract_in")
+    for rel, data in inputs.items():
+        os.makedirs(os.path.dirname(os.path.join(root, rel)), exist_ok=True)
+        with open(os.path.join(root, rel), "wb") as f:
+            f.write(data)
+    out = os.path.join(tmp, "extract_out.txt")
+    env = dict(os.environ, TMPDIR=os.path.join(tmp, "extract_tmp"))  # its fixed temp directory name
+    os.makedirs(env["TMPDIR"], exist_ok=True)
+    r = subprocess.run([os.path.join(REF_BIN, "ExtractOfftargets"), out, os.path.join(root, "g.fa"),
+                        os.path.join(root, "lines.txt"), os.path.join(root, "more")], env=env, capture_output=True,
+                       text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"ExtractOfftargets failed: {r.stderr[-2000:]}")
+    data = open(out, "rb").read()
+    arrays = {f"input_{i}": np.frombuffer(v, np.uint8) for i, v in enumerate(inputs.values())}
+    meta = {"name": "extract", "inputs": list(inputs), "args": ["g.fa", "lines.txt", "more"],
+            "output_sha256": hashlib.sha256(data).hexdigest(), "lines": data.count(b"\n")}
+    np.savez_compressed(os.path.join(HERE, "case_extract.npz"), meta=json.dumps(meta),
+                        output=np.frombuffer(data, np.uint8), **arrays)
+    print(f"extract: {meta['lines']} sites from {sum(len(v) for v in inputs.values())} input bytes")
+
+
 def main():
     mit, pos, pam = parse_penalties()
     hdr, legacy = legacy_mit_pairs()
@@ -353,6 +411,8 @@ def main():
             make_knife(tmp, pos, pam)
         if not only or "c0_full" in only:
             make_c0_full(tmp)
+        if not only or "extract" in only:
+            make_extract(tmp)
 
 
 if __name__ == "__main__":

@@ -1,9 +1,21 @@
 """The extraction oracle (oracle/extract_oracle.py) on hand-made inputs whose sites follow from
 the reference's rules by hand: forward and reverse patterns, overlaps, sequence breaks, FASTA
-records, plain-text lines, case and line endings. No GPU."""
+records, plain-text lines, case and line endings; and on the fixture made by the reference's own
+ExtractOfftargets. No GPU."""
 from __future__ import annotations
 
+import hashlib
+
 import extract_oracle as eo
+from conftest import extract_fixture
+
+
+def test_oracle_equals_reference_extractor(tmp_path):
+    """case_extract.npz holds the output of the reference's ExtractOfftargets (tests/golden/
+    make_golden.py): the restatement reproduces it byte for byte."""
+    paths, want, meta = extract_fixture(str(tmp_path))
+    assert hashlib.sha256(want).hexdigest() == meta["output_sha256"]
+    assert eo.extract_text(paths) == want
 
 F20 = "ACGTACGTACGTACGTACGT"
 

@@ -15,6 +15,17 @@ from conftest import REPO
 pytestmark = pytest.mark.gpu
 
 
+def test_extraction_equals_reference_extractor(native, tmp_path):
+    """The reference's own ExtractOfftargets output (case_extract.npz: FASTA with CRLF lines, N runs,
+    lower case and repeats, a plain file of lines, a directory), byte for byte."""
+    from conftest import extract_fixture
+    paths, want, meta = extract_fixture(str(tmp_path / "in"))
+    out = tmp_path / "out.txt"
+    n = native.extract_offtargets(paths, str(out))
+    assert n == meta["lines"]
+    assert out.read_bytes() == want
+
+
 def _genome(rng, n):
     s = np.array(list("ACGT"))[rng.choice(4, n, p=[0.295, 0.205, 0.205, 0.295])]
     s = "".join(s)

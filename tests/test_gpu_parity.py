@@ -78,6 +78,30 @@ def test_config0_full_size(native, tmp_path):
                                int(z["distinct_" + k][0]), tag=f"c0_full {k}")
 
 
+@pytest.mark.parametrize("spec", [
+    dict(seed=1235, n_sites=2_000_000, n_queries=2000),  # the benchmark's composition
+    dict(seed=7, n_sites=300_000, n_queries=600, repeat_frac=0.2, n_repeat_seeds=50, repeat_query_frac=0.2,
+         planted_into_sites=True),
+])
+def test_host_generator_equals_device_generator(native, oracle, spec):
+    """The benchmark's reference arm builds its index without the library: the oracle's host
+    restatement of the seeded generator (oracle/synth_oracle.c) must give the device generator's
+    sites, occurrence counts and guides exactly."""
+    ix, q = native.Index.synth(native.SynthSpec(slice_config="slice-8-20", **spec))
+    with ix:
+        sigs, _, _, lists = ix.export()
+    n = len(sigs)
+    occ = np.zeros(n, np.uint32)
+    occ[(lists[:n] & 0xFFFFFFFF).astype(np.int64)] = (lists[:n] >> 32).astype(np.uint32)
+    hs, ho, hq = oracle.synth(spec["seed"], spec["n_sites"], spec["n_queries"], repeat_frac=spec.get("repeat_frac", 0.05),
+                              n_repeat_seeds=spec.get("n_repeat_seeds", 10000), copied_frac=0.5,
+                              repeat_query_frac=spec.get("repeat_query_frac", 0.0),
+                              planted_into_sites=spec.get("planted_into_sites", False))
+    np.testing.assert_array_equal(hs, sigs)
+    np.testing.assert_array_equal(ho, occ)
+    np.testing.assert_array_equal(hq, q)
+
+
 def test_tiny_genome_from_reference_file(native):
     z, meta = load_case("tiny")
     with native.Index.open(os.path.join(GOLDEN, "tiny_genome.issl")) as ix:
@@ -377,3 +401,26 @@ def test_four_byte_entries_match(native, oracle_arrays, monkeypatch):
         assert ix8.info().entry_bytes == 8
         for a, b in zip(ix8.export(), oracle_arrays("c1_small")):
             np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["c4_small", "c2_small"])
+def test_capacity_path_conditions(native, oracle_arrays, monkeypatch, name):
+    """The conditions of the largest-index path on small cases: 4-byte list entries (signatures
+    read from the site table, which checks every scored site's distance independently of the
+    scan), guides scored in many chunks, and a range of scan unit sizes, staging depths, grids and
+    slice waves. Every call matches the reference fixtures and finds no site farther than 4
+    mismatches from its guide (a call that did would fail with ISSL_ERR_INTERNAL)."""
+    z, meta = load_case(name)
+    monkeypatch.setenv("ISSL_ENTRY_BYTES", "4")
+    monkeypatch.setenv("ISSL_MAX_GUIDES_PER_RUN", "37")
+    with native.Index.from_arrays(*oracle_arrays(name)) as ix:
+        assert ix.info().entry_bytes == 4
+        for chunk, stages, bps, fw in [((256, 256, 256), 2, 0, 0), ((512, 1024, 256), 4, 0, 2), ((1024, 512, 512), 3, 2, 1)]:
+            ix.set_tuning(chunk, stages, bps, fw)
+            for meth in meta["methods"]:
+                for t in [50.0, 99.9]:
+                    k = f"{meth}_{t}"
+                    res = ix.score(z["queries"], meth, t)
+                    assert_matches(res, z["mit_" + k], z["cfd_" + k], z["code_" + k].tobytes(), z["count_" + k],
+                                   int(z["distinct_" + k][0]), tag=f"{name} {k} {chunk} {stages} {bps} {fw}")
+                    assert ix.last_stats().dropped_hits == 0
