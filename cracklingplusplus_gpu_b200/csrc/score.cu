@@ -14,7 +14,8 @@
 //                   differs from the guide's in <= max_dist bases
 //   5 ownership     a candidate is kept only in the first slice that reaches it (replacing the
 //                   per-guide toggle bitset of :252-258): site reached in slice s is counted iff
-//                   no earlier slice has all its positions matching; counted per guide
+//                   no earlier slice has all its positions matching (from the site's list entry);
+//                   counted per guide
 //   6 hit offsets   per-guide hit counts -> segment offsets
 //   7 hit_scatter   hits grouped per guide: site id, occurrences and signature from the list entry
 //   8 score         per guide: exact fixed-point totals over the wave's hits plus the earlier
@@ -168,7 +169,7 @@ struct __align__(32) HitRec {
     double mit, cfd;
 };
 // device bytes per candidate slot: the candidate record and the grouped-hit record it may become
-constexpr size_t kCandSlotBytes = sizeof(uint4) + sizeof(HitRec);
+constexpr size_t kCandSlotBytes = sizeof(uint2) + sizeof(HitRec);
 
 struct issl::Workspace {
     int device = 0;
@@ -188,7 +189,7 @@ struct issl::Workspace {
     DevBuf<uint64_t> probe_qr;  // per probe slot: guide | residual << 32 (+2 padding)
     DevBuf<uint32_t> bucket_cnt, bucket_qstart, bucket_ustart;
     DevBuf<UnitDesc> units;
-    DevBuf<uint4> cands;  // candidate slots
+    DevBuf<uint2> cands;  // candidate slots: (guide | slice << 26, list position)
     DevBuf<HitRec> seg;   // owned hits grouped per guide
     DevBuf<uint32_t> qhits, qhoff, big, exitq;
     DevBuf<uint32_t> replayq;  // guides whose decision k_replay settles
@@ -486,9 +487,9 @@ __global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig,
 // (index, residual) pairs -- completing on the stage's mbarrier, while it computes unit t from
 // the stage that has landed. Lane l takes block l: per guide it forms the mismatch word of every
 // residual position (32 entries at once), adds them with a carry-save tree and keeps the entries
-// within max_dist. Candidates (rare) are written, with their residual mismatch mask, to slabs
-// of the candidate buffer that the warp reserves kCandSlab at a time; k_cand_own then applies the
-// ownership rule to the masks with every lane busy and no memory gathers.
+// within max_dist. Candidates (rare) are written as (guide | slice, list position) to slabs of the
+// candidate buffer that the warp reserves kCandSlab at a time; k_cand_own then reads each one's
+// list entry and applies the ownership rule with every lane busy.
 struct ScanArgs {
     const uint32_t* rbits;
     uint64_t rbits_base;  // global word number of rbits[0]
@@ -496,7 +497,7 @@ struct ScanArgs {
     const UnitDesc* units;
     const uint64_t* probe_qr;
     Counters* counters;
-    uint4* cands;
+    uint2* cands;
     uint32_t n_slices;
     uint32_t cand_cap;
     int max_dist;
@@ -509,23 +510,10 @@ struct ScanShared {  // per-block slice tables
     uint8_t wpb[kMaxSlices], rw[kMaxSlices];
 };
 
-// A warp's pending candidate records: lane i holds the i-th, and every 32 of them are written with
-// one reservation and one coalesced store.
-struct ScanCtx {
-    uint32_t x, y, z;  // this lane's pending record
-    uint32_t n;        // pending records in the warp (the same in every lane)
+struct ScanCtx {  // per-warp state of the candidate slab
+    uint32_t cpos, cend;
+    bool full;
 };
-
-__device__ __forceinline__ void flush_cands(const ScanArgs& a, ScanCtx& cx, int lane) {
-    if (!cx.n) return;
-    unsigned long long b = 0;
-    if (lane == 0) b = atomicAdd(&a.counters->cand_reserved, static_cast<unsigned long long>(cx.n));
-    b = __shfl_sync(0xffffffffu, b, 0);
-    // 64-bit reservations: a wave may ask for more slots than the buffer holds (the host then grows
-    // it, or splits the guides, and reruns); slots past the capacity are counted, never written
-    if (b + cx.n <= a.cand_cap && static_cast<uint32_t>(lane) < cx.n) a.cands[b + lane] = make_uint4(cx.x, cx.y, cx.z, 0u);
-    cx.n = 0;
-}
 
 // Compares every guide of the unit with the lane's block (RW residual positions per entry).
 template <int RW>
@@ -533,6 +521,7 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
                                           const StageMeta& m, uint32_t wpb, int lane, int max_dist, ScanCtx& cx) {
     constexpr int NW = 2 * RW;
     constexpr int NV = (NW + 3) / 4;
+    const unsigned lt = (1u << lane) - 1u;
     // this lane's block and the entries of it that belong to the unit (unsigned arithmetic: list
     // positions reach 2^32 - 1; the unit starts in block b0 and ends after this lane's block start)
     uint32_t d[NW];
@@ -577,41 +566,35 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
             if (2 * v < RW) mm[2 * v] = (d[4 * v] ^ w.x) | (d[4 * v + 1] ^ w.y);
             if (2 * v + 1 < RW) mm[2 * v + 1] = (d[4 * v + 2] ^ w.z) | (d[4 * v + 3] ^ w.w);
         }
-        const uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), max_dist) & valid;
-        // Candidates are rare. The warp takes them one at a time: lane p tests residual position p
-        // of the candidate's entry against the guide, straight from the staged block, and one
-        // ballot gives the candidate's residual mismatch mask (k_cand_own applies the ownership
-        // rule to it). Records are (guide | slice << 26, list position, mask).
-        unsigned hm = __ballot_sync(0xffffffffu, cbits != 0);
-        if (hm) {
-            uint32_t q0 = 0, q1 = 0;  // the guide's two bits at residual position `lane`, spread
-            if (lane < RW) {
-                const uint32_t rq = static_cast<uint32_t>(g >> 32);
-                q0 = 0u - ((rq >> (2 * lane)) & 1u);
-                q1 = 0u - ((rq >> (2 * lane + 1)) & 1u);
-            }
-            const uint32_t gx = static_cast<uint32_t>(g) | (m.s << kGuideBits);
-            do {
-                const int src = __ffs(hm) - 1;
-                hm &= hm - 1;
-                uint32_t cb = __shfl_sync(0xffffffffu, cbits, src);
-                uint32_t mw = 0;  // bit e: entry e of block src mismatches at position `lane`
-                if (lane < RW) {
-                    const uint32_t* sb = rb + m.delta + src * wpb;
-                    mw = (sb[2 * lane] ^ q0) | (sb[2 * lane + 1] ^ q1);
+        uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), max_dist) & valid;
+        // candidates are rare: one per lane per round, written to the warp's slab as (guide |
+        // slice << 26, list position); k_cand_own reads each one's list entry and applies the
+        // ownership rule to the site's mismatch positions
+        const uint32_t gx = static_cast<uint32_t>(g) | (m.s << kGuideBits);
+        for (unsigned hm = __ballot_sync(0xffffffffu, cbits != 0); hm; hm = __ballot_sync(0xffffffffu, cbits != 0)) {
+            const uint32_t nh = __popc(hm);
+            if (cx.cpos + nh > cx.cend) {
+                // retire the rest of the slab, reserve a new one
+                for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
+                    if (i < a.cand_cap) a.cands[i] = make_uint2(kDeadCand, 0);
+                // 64-bit reservations: a wave may ask for more than 2^32 slots (the host then splits
+                // the guides); a slab past the capacity is never written
+                uint32_t base = 0, full = 0;
+                if (lane == 0) {
+                    const unsigned long long b = atomicAdd(&a.counters->cand_reserved, static_cast<unsigned long long>(kCandSlab));
+                    full = b + kCandSlab > a.cand_cap;
+                    base = full ? a.cand_cap : static_cast<uint32_t>(b);
                 }
-                do {
-                    const int e = __ffs(cb) - 1;
-                    cb &= cb - 1;
-                    const uint32_t rmask = __ballot_sync(0xffffffffu, (mw >> e) & 1u);
-                    if (static_cast<uint32_t>(lane) == cx.n) {
-                        cx.x = gx;
-                        cx.y = 32u * (m.b0 + static_cast<uint32_t>(src)) + static_cast<uint32_t>(e);
-                        cx.z = rmask;
-                    }
-                    if (++cx.n == 32u) flush_cands(a, cx, lane);
-                } while (cb);
-            } while (hm);
+                cx.cpos = __shfl_sync(0xffffffffu, base, 0);
+                cx.cend = cx.cpos + kCandSlab;
+                cx.full = __shfl_sync(0xffffffffu, full, 0) != 0;
+            }
+            if (cbits) {
+                const int e = __ffs(cbits) - 1;
+                cbits &= cbits - 1;
+                if (!cx.full) a.cands[cx.cpos + __popc(hm & lt)] = make_uint2(gx, 32u * bl + e);
+            }
+            cx.cpos += nh;
         }
     }
 }
@@ -712,7 +695,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
         issued++;
     };
 
-    ScanCtx cx{0u, 0u, 0u, 0u};
+    ScanCtx cx{0u, 0u, false};
     for (uint32_t i = 0; i < NS; i++) try_issue();
     __syncwarp();
 
@@ -754,7 +737,8 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
         if (lane == 0) atomicOr(&a.counters->overflow, 4u);
         for (uint32_t u = t; u < issued; u++) mbar_wait_bounded(&bar[u % NS], (u / NS) & 1u, kWaitCycles);
     }
-    flush_cands(a, cx, lane);
+    for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
+        if (i < a.cand_cap) a.cands[i] = make_uint2(kDeadCand, 0);
 }
 
 __global__ void k_cands_finalize(Counters* c, uint32_t cand_cap) {
@@ -766,42 +750,41 @@ __global__ void k_cands_finalize(Counters* c, uint32_t cand_cap) {
 }
 
 // 5. the ownership rule on the candidates: a site reached in slice s is counted only if no
-// earlier slice has all its positions matching, i.e. every earlier slice mask meets the
-// mismatch positions (the residual mismatch mask spread back to protospacer positions).
-// Rejected slots are marked dead; owned ones are counted per guide.
-__global__ void k_cand_own(uint4* __restrict__ cands, const Counters* c, IndexView ix, uint32_t* __restrict__ qhits,
-                           const SetDesc* __restrict__ sets, const uint16_t* __restrict__ qset) {
-    __shared__ uint32_t s_pmask[kMaxSlices];
-    __shared__ uint8_t s_rpos[kMaxSlices][kSeqLen];
-    for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) {
-        s_pmask[i] = ix.geom[i].pmask;
-        for (int j = 0; j < kSeqLen; j++) s_rpos[i][j] = ix.geom[i].rpos[j];
-    }
+// earlier slice has all its positions matching, i.e. every earlier slice mask meets the site's
+// mismatch positions. Each candidate's list entry is read here (the scan only stores where the
+// candidate is): the site's signature gives its mismatch positions against the guide, and its
+// distance is checked against the bound the scan applied. Rejected slots are marked dead; owned
+// ones are counted per guide.
+__global__ void __launch_bounds__(256) k_cand_own(uint2* __restrict__ cands, Counters* c, IndexView ix,
+                                                   const uint64_t* __restrict__ qsig, uint32_t* __restrict__ qhits,
+                                                   const SetDesc* __restrict__ sets, const uint16_t* __restrict__ qset) {
+    __shared__ SliceGeom g[kMaxSlices];
+    for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
     __syncthreads();
     if (c->overflow) return;  // the host grows the buffers and reruns
     const uint32_t n = c->n_cand;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint4 r = cands[i];
+        const uint2 r = cands[i];
         if (r.x == kDeadCand) continue;
         const uint32_t s = r.x >> kGuideBits;
         const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
-        // batch form: the scan kept candidates up to the largest bound of the batch's sets; the
-        // residual mismatch count is the site's distance (the slice positions all match)
-        if (qset && __popc(r.z) > sets[qset[q]].P.max_dist) {
+        const uint64_t gq = qsig[q];
+        uint32_t id, occ;
+        uint64_t sig;
+        load_site(ix, s, r.y, gq, g[s], id, occ, sig);
+        const uint32_t mism20 = compress_even40(fold64(gq ^ sig));
+        const int dist = __popc(mism20);
+        if (dist > kMaxDist) {
+            // the scan found this site within the bound: a record that says otherwise does not
+            // describe a site of the guide's bucket (counted; the call then fails)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&c->dropped), 1ull);
             cands[i].x = kDeadCand;
             continue;
         }
-        uint32_t mism20 = 0, mm = r.z;
-        while (mm) {
-            mism20 |= 1u << s_rpos[s][__ffs(mm) - 1];
-            mm &= mm - 1;
-        }
-        bool own = true;
-        for (uint32_t e = 0; e < s; e++)
-            if ((mism20 & s_pmask[e]) == 0) {
-                own = false;  // an earlier slice reaches this site
-                break;
-            }
+        // batch form: the scan kept candidates up to the largest bound of the batch's sets
+        bool own = !(qset && dist > sets[qset[q]].P.max_dist);
+        for (uint32_t e = 0; e < s && own; e++)
+            if ((mism20 & g[e].pmask) == 0) own = false;  // an earlier slice reaches this site
         if (own)
             atomicAdd(&qhits[q], 1u);
         else
@@ -883,7 +866,7 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
 // guide's segment so that the scorers read only contiguous data.
 // (32 registers: eight blocks of 256 threads per SM keep the most random reads in flight)
 __global__ void __launch_bounds__(256, 8)
-    k_hit_scatter(const uint4* __restrict__ cands, Counters* c, uint32_t* __restrict__ qhits,
+    k_hit_scatter(const uint2* __restrict__ cands, Counters* c, uint32_t* __restrict__ qhits,
                   const uint32_t* __restrict__ qhoff, IndexView ix, const uint64_t* __restrict__ qsig,
                   const Tables* __restrict__ tables, HitRec* __restrict__ seg) {
     __shared__ SliceGeom g[kMaxSlices];
@@ -897,7 +880,7 @@ __global__ void __launch_bounds__(256, 8)
     both.calc_cfd = 1;
     const uint32_t n = c->n_cand;
     for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x) {
-        const uint4 r = cands[h];
+        const uint2 r = cands[h];
         if (r.x == kDeadCand) continue;
         const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
         const uint32_t sl = r.x >> kGuideBits;
@@ -1991,7 +1974,7 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         }
         if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[3 + 2 * w], st));
         k_cands_finalize<<<1, 1, 0, st>>>(C, sa.cand_cap);
-        k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, v, ws.qhits.p, R.sets, qset);
+        k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, v, R.qsig, ws.qhits.p, R.sets, qset);
         device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, d_n, n, ws.scan32.p, &C->hit_total,
                                      st);
         k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, ws.qhits.p, ws.qhoff.p, v, R.qsig, ws.tables.p,
@@ -2107,8 +2090,8 @@ void fill_stats(const Workspace& ws, float scan_ms, float total_ms, uint64_t lau
     s.buckets_scanned = ws.last.buckets;
     s.entries_scanned = ws.last.entries;
     // bytes the scan must move: the bit-sliced blocks it copies, 16 per unit descriptor, 8 per
-    // guide of a unit (index + residual), 16 per candidate slot written
-    s.scan_bytes = ws.last.rbytes + 16 * s.units + 8 * s.probes + 16 * ws.last.cands;
+    // guide of a unit (index + residual), 8 per candidate slot written
+    s.scan_bytes = ws.last.rbytes + 16 * s.units + 8 * s.probes + 8 * ws.last.cands;
     s.launches = launches;
     for (int i = 0; i < 3; i++) s.class_probes[i] = ws.last.class_probes[i];
     s.candidates = ws.last.cands;
