@@ -11,14 +11,15 @@
 //   3 probe_scatter guides grouped by bucket, with each guide's residual code for that slice
 //   4 scan          persistent, work-stealing: stream the bit-sliced residual codes of every unit
 //                   through per-warp bulk-copy rings; a candidate is an entry whose residual
-//                   differs from the guide's in <= max_dist bases
-//   5 ownership     a candidate is kept only in the first slice that reaches it (replacing the
-//                   per-guide toggle bitset of :252-258): site reached in slice s is counted iff
-//                   no earlier slice has all its positions matching (from the site's list entry);
-//                   counted per guide
-//   6 hit offsets   per-guide hit counts -> segment offsets
-//   7 hit_scatter   hits grouped per guide: site id, occurrences and signature from the list entry
-//   8 score         per guide: exact fixed-point totals over the wave's hits plus the earlier
+//                   differs from the guide's in <= max_dist bases; candidates are counted per guide
+//   5 segments      the exclusive prefix of the per-guide candidate counts: each guide's segment
+//                   of the hit buffer
+//   6 resolve       per candidate: its list entry (site id, occurrences, signature); kept only in
+//                   the first slice that reaches it (replacing the per-guide toggle bitset of
+//                   :252-258): a site reached in slice s counts iff no earlier slice has all its
+//                   positions matching; the kept ones get their MIT and CFD contributions and go
+//                   to the next free slot of their guide's segment
+//   7 score         per guide: exact fixed-point totals over the wave's hits plus the earlier
 //                   waves'; guides whose early-exit test (:366-395) fires are ordered as the
 //                   reference visits them (slice, then list position) to find the exact stop;
 //                   the others are finalised (:404-459) after the last wave or carried on
@@ -60,7 +61,7 @@ struct Counters {
     unsigned long long cand_reserved;  // candidate slots reserved by the scan (may exceed capacity)
     uint32_t n_units;       // min(units, capacity)
     uint32_t n_cand;        // min(cand_reserved, capacity): the slots the later kernels read
-    uint32_t hit_total;     // owned hits: sum of per-guide hits (scan total)
+    uint32_t hit_total;     // owned hits of the wave (the resolve pass counts them)
     uint32_t n_big;         // exiting guides with more than kWarpSort hits (block scorer)
     uint32_t n_exit;        // exiting guides with at most kWarpSort hits (warp scorer)
     uint32_t next_batch;    // work queue of the scan: next batch of 32 units to take
@@ -181,7 +182,7 @@ struct issl::Workspace {
     int scan_rw = 0;  // residual width the scan is specialised for (0: mixed)
     WarpLayout scan_layout{};
     int scan_smem = 0;
-    bool zero_state_ok = false;  // bucket_cnt / qhits are all zero between calls
+    bool zero_state_ok = false;  // bucket_cnt is all zero between calls
     DevBuf<uint64_t> qsig;
     DevBuf<char> ascii;
     size_t ascii_cap = 0;
@@ -191,7 +192,8 @@ struct issl::Workspace {
     DevBuf<UnitDesc> units;
     DevBuf<uint2> cands;  // candidate slots: (guide | slice << 26, list position)
     DevBuf<HitRec> seg;   // owned hits grouped per guide
-    DevBuf<uint32_t> qhits, qhoff, big, exitq;
+    // per guide: candidates of the wave (counted by the scan), segment start, owned hits written
+    DevBuf<uint32_t> qcand, qoff, qfill, big, exitq;
     DevBuf<uint32_t> replayq;  // guides whose decision k_replay settles
     DevBuf<uint32_t> bitmap;
     DevBuf<Counters> counters;
@@ -313,11 +315,11 @@ struct BucketLoad {
         const uint64_t g = g0 + gi;
         const uint32_t c = cnt[g];
         if (!c) return 0;
-        // chunks are aligned to the chunk size within the slice (which divides kChunk), so a
-        // unit never spans two kChunk blocks
+        // a unit is up to C / 32 consecutive 32-entry blocks, counted from the bucket's first
+        // block, so it never spans more than 32 blocks (one per lane)
         const uint64_t C = chunk_of(off[g + 1] - off[g], cc);
         const uint64_t sb = (off[g] / n_sites) * n_sites;
-        const uint64_t chunks = (off[g + 1] - 1 - sb) / C - (off[g] - sb) / C + 1;
+        const uint64_t chunks = (((off[g + 1] - 1 - sb) >> 5) - ((off[g] - sb) >> 5)) / (C >> 5) + 1;
         const uint64_t units = chunks * ((c + kGroup - 1) / kGroup);
         return (units << 32) | c;
     }
@@ -401,9 +403,12 @@ __global__ void k_expand_units(const uint32_t* __restrict__ cnt, const uint64_t*
             }
             const uint32_t r = static_cast<uint32_t>(u) - u0;
             const uint32_t k = r / ng, j = r - k * ng;
-            const uint64_t blk = (e0 >> lc) + k;
-            const uint64_t cb = (blk << lc) > e0 ? (blk << lc) : e0;
-            const uint64_t ce = ((blk + 1) << lc) < e1 ? ((blk + 1) << lc) : e1;
+            // unit k: blocks [B0 + k * C/32, B0 + (k + 1) * C/32) of the bucket, B0 its first block
+            const uint64_t B0 = e0 >> 5;
+            const uint64_t first = (B0 + (static_cast<uint64_t>(k) << (lc - 5))) << 5;
+            const uint64_t last = (B0 + (static_cast<uint64_t>(k + 1) << (lc - 5))) << 5;
+            const uint64_t cb = first > e0 ? first : e0;
+            const uint64_t ce = last < e1 ? last : e1;
             UnitDesc d;
             d.p0 = static_cast<uint32_t>(cb);
             d.qbeg = q0 + j * kGroup;
@@ -488,7 +493,7 @@ __global__ void k_probe_scatter(IndexView ix, const uint64_t* __restrict__ qsig,
 // the stage that has landed. Lane l takes block l: per guide it forms the mismatch word of every
 // residual position (32 entries at once), adds them with a carry-save tree and keeps the entries
 // within max_dist. Candidates (rare) are written as (guide | slice, list position) to slabs of the
-// candidate buffer that the warp reserves kCandSlab at a time; k_cand_own then reads each one's
+// candidate buffer that the warp reserves kCandSlab at a time; k_cand_resolve then reads each one's
 // list entry and applies the ownership rule with every lane busy.
 struct ScanArgs {
     const uint32_t* rbits;
@@ -498,6 +503,7 @@ struct ScanArgs {
     const uint64_t* probe_qr;
     Counters* counters;
     uint2* cands;
+    uint32_t* qcand;      // candidates per guide (sizes the guides' hit segments)
     uint32_t n_slices;
     uint32_t cand_cap;
     int max_dist;
@@ -568,11 +574,12 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
         }
         uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), max_dist) & valid;
         // candidates are rare: one per lane per round, written to the warp's slab as (guide |
-        // slice << 26, list position); k_cand_own reads each one's list entry and applies the
-        // ownership rule to the site's mismatch positions
+        // slice << 26, list position) and counted per guide; k_cand_resolve reads each one's list
+        // entry and applies the ownership rule to the site's mismatch positions
         const uint32_t gx = static_cast<uint32_t>(g) | (m.s << kGuideBits);
         for (unsigned hm = __ballot_sync(0xffffffffu, cbits != 0); hm; hm = __ballot_sync(0xffffffffu, cbits != 0)) {
             const uint32_t nh = __popc(hm);
+            if (lane == 0) atomicAdd(&a.qcand[static_cast<uint32_t>(g)], nh);
             if (cx.cpos + nh > cx.cend) {
                 // retire the rest of the slab, reserve a new one
                 for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
@@ -749,51 +756,10 @@ __global__ void k_cands_finalize(Counters* c, uint32_t cand_cap) {
     c->n_cand = static_cast<uint32_t>(r < cand_cap ? r : cand_cap);
 }
 
-// 5. the ownership rule on the candidates: a site reached in slice s is counted only if no
-// earlier slice has all its positions matching, i.e. every earlier slice mask meets the site's
-// mismatch positions. Each candidate's list entry is read here (the scan only stores where the
-// candidate is): the site's signature gives its mismatch positions against the guide, and its
-// distance is checked against the bound the scan applied. Rejected slots are marked dead; owned
-// ones are counted per guide.
-__global__ void __launch_bounds__(256) k_cand_own(uint2* __restrict__ cands, Counters* c, IndexView ix,
-                                                   const uint64_t* __restrict__ qsig, uint32_t* __restrict__ qhits,
-                                                   const SetDesc* __restrict__ sets, const uint16_t* __restrict__ qset) {
-    __shared__ SliceGeom g[kMaxSlices];
-    for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
-    __syncthreads();
-    if (c->overflow) return;  // the host grows the buffers and reruns
-    const uint32_t n = c->n_cand;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint2 r = cands[i];
-        if (r.x == kDeadCand) continue;
-        const uint32_t s = r.x >> kGuideBits;
-        const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
-        const uint64_t gq = qsig[q];
-        uint32_t id, occ;
-        uint64_t sig;
-        load_site(ix, s, r.y, gq, g[s], id, occ, sig);
-        const uint32_t mism20 = compress_even40(fold64(gq ^ sig));
-        const int dist = __popc(mism20);
-        if (dist > kMaxDist) {
-            // the scan found this site within the bound: a record that says otherwise does not
-            // describe a site of the guide's bucket (counted; the call then fails)
-            atomicAdd(reinterpret_cast<unsigned long long*>(&c->dropped), 1ull);
-            cands[i].x = kDeadCand;
-            continue;
-        }
-        // batch form: the scan kept candidates up to the largest bound of the batch's sets
-        bool own = !(qset && dist > sets[qset[q]].P.max_dist);
-        for (uint32_t e = 0; e < s && own; e++)
-            if ((mism20 & g[e].pmask) == 0) own = false;  // an earlier slice reaches this site
-        if (own)
-            atomicAdd(&qhits[q], 1u);
-        else
-            cands[i].x = kDeadCand;
-    }
-}
-
 // ---------------------------------------------------------------------------------------------
-// 6. hits grouped per guide
+// 5. per-guide segments: the scan counts each guide's candidates; their exclusive prefix gives
+// every guide a segment of the hit buffer large enough for all of them, which the resolve pass
+// fills from its start with the candidates that survive the ownership rule
 struct LoadQhits {
     const uint32_t* p;
     __device__ uint32_t operator()(uint64_t i) const { return p[i]; }
@@ -859,50 +825,64 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
     return c;
 }
 
-// One thread per owned hit (many independent loads in flight): the list entry gives the site id,
-// its occurrences and (8-byte entries) its residual code, from which the signature is rebuilt;
-// with 4-byte entries the signature is a second read. The hit's MIT and CFD contributions are
-// computed here, where the random reads leave the arithmetic units idle, and written into the
-// guide's segment so that the scorers read only contiguous data.
-// (32 registers: eight blocks of 256 threads per SM keep the most random reads in flight)
-__global__ void __launch_bounds__(256, 8)
-    k_hit_scatter(const uint2* __restrict__ cands, Counters* c, uint32_t* __restrict__ qhits,
-                  const uint32_t* __restrict__ qhoff, IndexView ix, const uint64_t* __restrict__ qsig,
-                  const Tables* __restrict__ tables, HitRec* __restrict__ seg) {
+// 6. One thread per candidate (many independent random reads in flight). The list entry gives the
+// site id, its occurrences and (8-byte entries) its residual code, from which the signature is
+// rebuilt; with 4-byte entries the signature is a second read. The site's mismatch positions
+// against the guide then settle the ownership rule (a site reached in slice s is counted only if
+// no earlier slice has all its positions matching, the reference's toggle bitset of :252-258):
+// avoid[p] holds the slices that do not contain position p, so the slices whose positions all
+// match the site are the AND of avoid[] over its (at most four) mismatch positions. An owned site's
+// MIT and CFD contributions are computed here, where the reads leave the arithmetic units idle, and
+// its record is written to the next free slot of its guide's segment, so the scorers read only
+// contiguous data.
+__global__ void __launch_bounds__(256)
+    k_cand_resolve(const uint2* __restrict__ cands, Counters* c, IndexView ix, const uint64_t* __restrict__ qsig,
+                   const uint32_t* __restrict__ qoff, uint32_t* __restrict__ qfill, const Tables* __restrict__ tables,
+                   HitRec* __restrict__ seg, const SetDesc* __restrict__ sets, const uint16_t* __restrict__ qset) {
     __shared__ SliceGeom g[kMaxSlices];
+    __shared__ unsigned long long avoid[kSeqLen];
     for (int i = threadIdx.x; i < static_cast<int>(ix.n_slices); i += blockDim.x) g[i] = ix.geom[i];
+    if (threadIdx.x < kSeqLen) {
+        unsigned long long m = 0;
+        for (uint32_t e = 0; e < ix.n_slices; e++)
+            if (!((ix.geom[e].pmask >> threadIdx.x) & 1u)) m |= 1ull << e;
+        avoid[threadIdx.x] = m;
+    }
     __syncthreads();
-    if (blockIdx.x == 0 && threadIdx.x == 0) c->hits += c->hit_total;
-    if (c->overflow) return;
+    if (c->overflow) return;  // the host grows the buffers and reruns
     const Tables& T = *tables;
     ScoreParams both{};
     both.calc_mit = 1;
     both.calc_cfd = 1;
     const uint32_t n = c->n_cand;
-    for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x) {
-        const uint2 r = cands[h];
+    uint32_t owned_here = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint2 r = cands[i];
         if (r.x == kDeadCand) continue;
+        const uint32_t s = r.x >> kGuideBits;
         const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
-        const uint32_t sl = r.x >> kGuideBits;
         const uint64_t gq = qsig[q];
         uint32_t id, occ;
         uint64_t sig;
-        load_site(ix, sl, r.y, gq, g[sl], id, occ, sig);
-        // A scored site is within kMaxDist of the guide by construction (its slice positions
-        // match and the scan bounds the rest). Should a record ever say otherwise, it counts for
-        // nothing here (no occurrences, no scores, no distinct site, and the MIT table is never
-        // indexed out of range) and the call fails with ISSL_ERR_INTERNAL.
-        Contribution ct = contribution(T, both, gq, sig, occ);
+        load_site(ix, s, r.y, gq, g[s], id, occ, sig);
+        const Contribution ct = contribution(T, both, gq, sig, occ);
         if (ct.dist > kMaxDist) {
-            ct.mit = ct.cfd = 0.0;
-            occ = 0;
-            id = kNoSite;
+            // the scan found this site within the bound: a record that says otherwise does not
+            // describe a site of the guide's bucket (counted; the call then fails)
             atomicAdd(reinterpret_cast<unsigned long long*>(&c->dropped), 1ull);
+            continue;
         }
-        // the decrement leaves qhits all zero for the next call
-        const uint32_t slot = qhoff[q] + atomicSub(&qhits[q], 1u) - 1u;
-        seg[slot] = HitRec{make_uint4(r.y, sl, id, occ), ct.mit, ct.cfd};
+        // batch form: the scan kept candidates up to the largest bound of the batch's sets
+        if (qset && ct.dist > sets[qset[q]].P.max_dist) continue;
+        unsigned long long reach = ~0ull;  // slices whose positions all match the site
+        for (uint32_t mm = compress_even40(fold64(gq ^ sig)); mm; mm &= mm - 1) reach &= avoid[__ffs(mm) - 1];
+        if (reach & ((1ull << s) - 1ull)) continue;  // an earlier slice reaches this site
+        const uint32_t slot = qoff[q] + atomicAdd(&qfill[q], 1u);
+        seg[slot] = HitRec{make_uint4(r.y, s, id, occ), ct.mit, ct.cfd};
+        owned_here++;
     }
+    for (int d = 16; d > 0; d >>= 1) owned_here += __shfl_xor_sync(0xffffffffu, owned_here, d);
+    if ((threadIdx.x & 31) == 0 && owned_here) atomicAdd(&c->hit_total, owned_here);
 }
 
 __device__ __forceinline__ bool exit_test(const ScoreParams& P, double mit, double cfd) {
@@ -980,14 +960,6 @@ __device__ __forceinline__ bool settled_at_exit(const ScoreParams& P, double pm,
            rejects(P, sm.lo, sc.lo) == rejects(P, sm.hi, sc.hi);
 }
 
-__device__ __forceinline__ double warp_incl_sum(double v, int lane) {
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const double o = __shfl_up_sync(0xffffffffu, v, d);
-        if (lane >= d) v += o;
-    }
-    return v;
-}
 __device__ __forceinline__ uint64_t warp_incl_sum_u64(uint64_t v, int lane) {
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -1003,7 +975,8 @@ struct ScoreArgs {
     IndexView ix;
     const uint64_t* qsig;
     HitRec* seg;
-    const uint32_t* qhoff;
+    const uint32_t* qoff;    // each guide's hit segment: start, and hits written
+    const uint32_t* qfill;
     const Tables* tables;
     Counters* counters;
     uint32_t* big;
@@ -1105,13 +1078,14 @@ constexpr int kWarpSort = 1024;  // exiting guides with more hits are ordered by
 // test fires go to the ordered scorers.
 __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.counters->hits += a.counters->hit_total;
     if (a.counters->overflow) return;  // rerun follows
     const uint64_t gw = blockIdx.x * 8ull + warp, nw = gridDim.x * 8ull;
     const uint64_t n = a.d_nact ? *a.d_nact : guide_count(a.d_n, a.n);
     for (uint64_t i = gw; i < n; i += nw) {
         const uint64_t qi = a.active ? a.active[i] : i;
         const ScoreParams P = params_of(a, qi);
-        const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
+        const uint32_t h0 = a.qoff[qi], L = a.qfill[qi];
         const HitRec* seg = a.seg + h0;
         Fx tm{0, 0}, tc{0, 0};
         uint64_t tn = 0;
@@ -1194,7 +1168,7 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
             rc = pr.cfd;
             rn = pr.occ;
         }
-        const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
+        const uint32_t h0 = a.qoff[qi], L = a.qfill[qi];
         const HitRec* seg = a.seg + h0;
         // counting sort of the hits by slice
         for (uint32_t t = lane; t <= S; t += 32) W.cnt[t] = 0;
@@ -1353,7 +1327,7 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             run_c = pr.cfd;
             run_n = pr.occ;
         }
-        const uint32_t h0 = a.qhoff[qi], L = a.qhoff[qi + 1] - h0;
+        const uint32_t h0 = a.qoff[qi], L = a.qfill[qi];
         HitRec* seg = a.seg + h0;
         uint32_t P2 = 1;
         while (P2 < L) P2 <<= 1;
@@ -1745,13 +1719,14 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
         ws.g_cap = G + 1;
         ws.epoch++;
     }
-    if (ws.q_cap < n || !ws.qhits.p) {
+    if (ws.q_cap < n || !ws.qcand.p) {
         const size_t cap = std::max<size_t>(n, 1024);
         ws.qsig.reserve(cap);
         ws.probe_gb.reserve(cap * S);
         ws.probe_qr.reserve(cap * S + 2);
-        ws.qhits.reserve(cap + 1);
-        ws.qhoff.reserve(cap + 1);
+        ws.qcand.reserve(cap + 1);
+        ws.qoff.reserve(cap + 1);
+        ws.qfill.reserve(cap + 1);
         ws.big.reserve(cap);
         ws.exitq.reserve(cap);
         ws.replayq.reserve(cap);
@@ -1764,7 +1739,6 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
         ws.active[1].reserve(cap);
         ws.acc.reserve(cap * 5);
         if (ws.qset.p) ws.qset.reserve(cap);
-        ISSL_CUDA(cudaMemsetAsync(ws.qhits.p, 0, (cap + 1) * 4, st));
         ws.q_cap = cap;
         ws.epoch++;
     }
@@ -1774,7 +1748,6 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
     }
     if (!ws.zero_state_ok) {
         ISSL_CUDA(cudaMemsetAsync(ws.bucket_cnt.p, 0, (G + 1) * 4, st));
-        ISSL_CUDA(cudaMemsetAsync(ws.qhits.p, 0, (ws.q_cap + 1) * 4, st));
         ws.zero_state_ok = true;
     }
     // first guesses: ~2.5 units per probe with 1024-entry units (more with smaller ones) plus
@@ -1816,7 +1789,7 @@ void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide,
              (65536 + slab_slack) * *per_candidate;
     // qsig, probe lists, hit counts and offsets, exit and replay queues, outputs, set map, wave
     // lists and running totals; scan units
-    *per_guide = 8 + 12 * S + 5 * 4 + (8 + 8 + 1 + 8) + 2 + 2 * 4 + 5 * 8 +
+    *per_guide = 8 + 12 * S + 6 * 4 + (8 + 8 + 1 + 8) + 2 + 2 * 4 + 5 * 8 +
                  sizeof(UnitDesc) * 3 * S * (kChunk / min_chunk);
     uint64_t idw, cw;  // the two slice windows of a host-list index
     window_capacity(ix, &idw, &cw);
@@ -1935,6 +1908,8 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
             v.rbits_base = wbase0;
         }
         if (!first) ISSL_CUDA(cudaMemsetAsync(C, 0, kWaveCounterBytes, st));
+        ISSL_CUDA(cudaMemsetAsync(ws.qcand.p, 0, (n + 1) * 4, st));
+        ISSL_CUDA(cudaMemsetAsync(ws.qfill.p, 0, (n + 1) * 4, st));
         if (!last) ISSL_CUDA(cudaMemsetAsync(&C->act_n[nxt], 0, 4, st));
         const WaveProbes wp{first ? nullptr : ws.active[cur].p, first ? nullptr : &C->act_n[cur], d_n, n, s0, s1 - s0};
         const uint64_t g0 = ix->geom[s0].bbase, g1 = s1 < S ? ix->geom[s1].bbase : G;
@@ -1959,6 +1934,7 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         sa.probe_qr = ws.probe_qr.p;
         sa.counters = C;
         sa.cands = ws.cands.p;
+        sa.qcand = ws.qcand.p;
         sa.n_slices = static_cast<uint32_t>(S);
         sa.cand_cap = static_cast<uint32_t>(std::min<size_t>(ws.cand_cap, 0xFFFFFFFFull));
         sa.max_dist = R.P.max_dist;
@@ -1974,20 +1950,20 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         }
         if (R.events) ISSL_CUDA(cudaEventRecord(ws.ev[3 + 2 * w], st));
         k_cands_finalize<<<1, 1, 0, st>>>(C, sa.cand_cap);
-        k_cand_own<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, v, R.qsig, ws.qhits.p, R.sets, qset);
-        device_scan<uint32_t, OpSum>(LoadQhits{ws.qhits.p}, StoreQoff{ws.qhoff.p}, d_n, n, ws.scan32.p, &C->hit_total,
-                                     st);
-        k_hit_scatter<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, ws.qhits.p, ws.qhoff.p, v, R.qsig, ws.tables.p,
-                                               ws.seg.p);
+        // each guide's segment of the hit buffer: the exclusive prefix of its candidate count
+        device_scan<uint32_t, OpSum>(LoadQhits{ws.qcand.p}, StoreQoff{ws.qoff.p}, d_n, n, ws.scan32.p, nullptr, st);
+        k_cand_resolve<<<sms * 8, 256, 0, st>>>(ws.cands.p, C, v, R.qsig, ws.qoff.p, ws.qfill.p, ws.tables.p, ws.seg.p,
+                                                R.sets, qset);
         if (staged) ISSL_CUDA(cudaEventRecord(ws.win_free[wb], st));  // the last reader of the window
-        k += 7;
+        k += 6;
         ScoreArgs a;
         a.ix = v;
         a.qsig = R.qsig;
         a.seg = ws.seg.p;
         a.exitq = ws.exitq.p;
         a.replay = ws.replayq.p;
-        a.qhoff = ws.qhoff.p;
+        a.qoff = ws.qoff.p;
+        a.qfill = ws.qfill.p;
         a.tables = ws.tables.p;
         a.counters = C;
         a.big = ws.big.p;
@@ -2717,7 +2693,6 @@ __global__ void __launch_bounds__(kStaticThreads) k_score_static(StaticArgs a) {
     __shared__ int s_stop;
     for (int i = threadIdx.x; i < static_cast<int>(a.ix.n_slices); i += blockDim.x) s_geom[i] = a.ix.geom[i];
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const Tables& T = *a.tables;
     uint4* hits = a.hits + static_cast<size_t>(blockIdx.x) * kStaticHits;
     for (uint64_t qi = blockIdx.x; qi < a.n; qi += gridDim.x) {
