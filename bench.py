@@ -318,11 +318,13 @@ def run_ours(args):
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
+    torch.cuda.nvtx.range_push("timed_e2e")
     t0 = time.perf_counter()
     for _ in range(args.steps):
         step_e2e()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
+    torch.cuda.nvtx.range_pop()
     if world > 1:
         e2e_s = max_over_ranks(e2e_s, dev)
     e2e_value = whole_job_rate(world, nq, args.steps, e2e_s)
