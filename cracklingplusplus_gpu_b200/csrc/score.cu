@@ -548,27 +548,25 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
     // written while this guide's are read, one warp barrier per guide
     if (m.qn) {
         const uint32_t rq0 = static_cast<uint32_t>(qr[m.qoff] >> 32);
-        __syncwarp();
+        __syncwarp();  // the previous unit's reads of the mask buffers are done
         if (lane < NW) qm[lane] = 0u - ((rq0 >> lane) & 1u);
-        __syncwarp();
     }
     for (uint32_t k = 0; k < m.qn; k++) {
+        // this guide's masks are complete; the other buffer's last reads (the previous guide's)
+        // are done, so it takes the next guide's masks while this one's are read
+        __syncwarp();
         const uint64_t g = qr[m.qoff + k];
-        // guide masks come as 128-bit broadcast reads, two positions per read
-        const uint4* qm4 = reinterpret_cast<const uint4*>(qm + 32u * (k & 1u));
-        uint4 wv[NV];
-#pragma unroll
-        for (int v = 0; v < NV; v++) wv[v] = qm4[v];
         if (k + 1 < m.qn) {
             const uint32_t rqn = static_cast<uint32_t>(qr[m.qoff + k + 1] >> 32);
             if (lane < NW) qm[32u * ((k + 1) & 1u) + lane] = 0u - ((rqn >> lane) & 1u);
         }
-        __syncwarp();  // the other buffer is complete; this one's reads are done
-        // mismatch word of each residual position
+        // mismatch word of each residual position; guide masks come as 128-bit broadcast reads,
+        // two positions per read
+        const uint4* qm4 = reinterpret_cast<const uint4*>(qm + 32u * (k & 1u));
         uint32_t mm[RW];
 #pragma unroll
         for (int v = 0; v < NV; v++) {
-            const uint4 w = wv[v];
+            const uint4 w = qm4[v];
             if (2 * v < RW) mm[2 * v] = (d[4 * v] ^ w.x) | (d[4 * v + 1] ^ w.y);
             if (2 * v + 1 < RW) mm[2 * v + 1] = (d[4 * v + 2] ^ w.z) | (d[4 * v + 3] ^ w.w);
         }
