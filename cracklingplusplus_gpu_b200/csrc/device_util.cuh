@@ -50,6 +50,14 @@ __device__ __forceinline__ void load_site(const IndexView& v, uint32_t s, uint32
     }
 }
 
+// The raw list entry of list position `pos` of slice s: the packed id (x) and, with 8-byte entries,
+// the residual code (y; 0 with 4-byte entries).
+__device__ __forceinline__ uint2 load_entry(const IndexView& v, uint32_t s, uint32_t pos) {
+    const uint64_t j = static_cast<uint64_t>(s) * v.n_sites + pos - v.ids_base;
+    if (v.entry_words == 2) return reinterpret_cast<const uint2*>(v.ids)[j];
+    return make_uint2(v.ids[j], 0u);
+}
+
 // One bit per mismatching base pair, at the even bit of each 2-bit field. Equivalent to
 // ((x & 0xAA..) >> 1) | (x & 0x55..) of ISSLScoringModule.cpp:287-289.
 __host__ __device__ __forceinline__ uint64_t fold64(uint64_t x) {

@@ -833,7 +833,7 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
 // MIT and CFD contributions are computed here, where the reads leave the arithmetic units idle, and
 // its record is written to the next free slot of its guide's segment, so the scorers read only
 // contiguous data.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 5)
     k_cand_resolve(const uint2* __restrict__ cands, Counters* c, IndexView ix, const uint64_t* __restrict__ qsig,
                    const uint32_t* __restrict__ qoff, uint32_t* __restrict__ qfill, const Tables* __restrict__ tables,
                    HitRec* __restrict__ seg, const SetDesc* __restrict__ sets, const uint16_t* __restrict__ qset) {
@@ -848,36 +848,57 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
     if (c->overflow) return;  // the host grows the buffers and reruns
-    const Tables& T = *tables;
+    const Tables& T_ = *tables;
     ScoreParams both{};
     both.calc_mit = 1;
     both.calc_cfd = 1;
     const uint32_t n = c->n_cand;
     uint32_t owned_here = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint2 r = cands[i];
-        if (r.x == kDeadCand) continue;
-        const uint32_t s = r.x >> kGuideBits;
-        const uint32_t q = r.x & ((1u << kGuideBits) - 1u);
-        const uint64_t gq = qsig[q];
-        uint32_t id, occ;
-        uint64_t sig;
-        load_site(ix, s, r.y, gq, g[s], id, occ, sig);
-        const Contribution ct = contribution(T, both, gq, sig, occ);
-        if (ct.dist > kMaxDist) {
-            // the scan found this site within the bound: a record that says otherwise does not
-            // describe a site of the guide's bucket (counted; the call then fails)
-            atomicAdd(reinterpret_cast<unsigned long long*>(&c->dropped), 1ull);
-            continue;
+    // two candidates per thread and round, their reads issued together (the random list-entry
+    // reads are the bound: more of them in flight per thread)
+    constexpr int U = 2;
+    const uint32_t T = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * T) {
+        uint2 r[U];
+        uint64_t gq[U];
+        uint2 e[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint32_t i = i0 + u * T;
+            r[u] = i < n ? cands[i] : make_uint2(kDeadCand, 0u);
         }
-        // batch form: the scan kept candidates up to the largest bound of the batch's sets
-        if (qset && ct.dist > sets[qset[q]].P.max_dist) continue;
-        unsigned long long reach = ~0ull;  // slices whose positions all match the site
-        for (uint32_t mm = compress_even40(fold64(gq ^ sig)); mm; mm &= mm - 1) reach &= avoid[__ffs(mm) - 1];
-        if (reach & ((1ull << s) - 1ull)) continue;  // an earlier slice reaches this site
-        const uint32_t slot = qoff[q] + atomicAdd(&qfill[q], 1u);
-        seg[slot] = HitRec{make_uint4(r.y, s, id, occ), ct.mit, ct.cfd};
-        owned_here++;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (r[u].x == kDeadCand) continue;
+            gq[u] = qsig[r[u].x & ((1u << kGuideBits) - 1u)];
+            e[u] = load_entry(ix, r[u].x >> kGuideBits, r[u].y);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (r[u].x == kDeadCand) continue;
+            const uint32_t s = r[u].x >> kGuideBits;
+            const uint32_t q = r[u].x & ((1u << kGuideBits) - 1u);
+            const uint32_t id = entry_id(e[u].x, ix.id_bits);
+            const uint64_t sig = ix.entry_words == 2 ? site_signature(gq[u], e[u].y, g[s]) : ix.sigs[id];
+            const uint32_t mism20 = compress_even40(fold64(gq[u] ^ sig));
+            const int dist = __popc(mism20);
+            if (dist > kMaxDist) {
+                // the scan found this site within the bound: a record that says otherwise does not
+                // describe a site of the guide's bucket (counted; the call then fails)
+                atomicAdd(reinterpret_cast<unsigned long long*>(&c->dropped), 1ull);
+                continue;
+            }
+            // batch form: the scan kept candidates up to the largest bound of the batch's sets
+            if (qset && dist > sets[qset[q]].P.max_dist) continue;
+            unsigned long long reach = ~0ull;  // slices whose positions all match the site
+            for (uint32_t mm = mism20; mm; mm &= mm - 1) reach &= avoid[__ffs(mm) - 1];
+            if (reach & ((1ull << s) - 1ull)) continue;  // an earlier slice reaches this site
+            const uint32_t occ = entry_occ(e[u].x, ix);
+            const Contribution ct = contribution(T_, both, gq[u], sig, occ);
+            const uint32_t slot = qoff[q] + atomicAdd(&qfill[q], 1u);
+            seg[slot] = HitRec{make_uint4(r[u].y, s, id, occ), ct.mit, ct.cfd};
+            owned_here++;
+        }
     }
     for (int d = 16; d > 0; d >>= 1) owned_here += __shfl_xor_sync(0xffffffffu, owned_here, d);
     if ((threadIdx.x & 31) == 0 && owned_here) atomicAdd(&c->hit_total, owned_here);
