@@ -833,7 +833,7 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
 // MIT and CFD contributions are computed here, where the reads leave the arithmetic units idle, and
 // its record is written to the next free slot of its guide's segment, so the scorers read only
 // contiguous data.
-__global__ void __launch_bounds__(256, 5)
+__global__ void __launch_bounds__(256, 4)
     k_cand_resolve(const uint2* __restrict__ cands, Counters* c, IndexView ix, const uint64_t* __restrict__ qsig,
                    const uint32_t* __restrict__ qoff, uint32_t* __restrict__ qfill, const Tables* __restrict__ tables,
                    HitRec* __restrict__ seg, const SetDesc* __restrict__ sets, const uint16_t* __restrict__ qset) {
@@ -854,9 +854,9 @@ __global__ void __launch_bounds__(256, 5)
     both.calc_cfd = 1;
     const uint32_t n = c->n_cand;
     uint32_t owned_here = 0;
-    // two candidates per thread and round, their reads issued together (the random list-entry
+    // four candidates per thread and round, their reads issued together (the random list-entry
     // reads are the bound: more of them in flight per thread)
-    constexpr int U = 2;
+    constexpr int U = 4;
     const uint32_t T = gridDim.x * blockDim.x;
     for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * T) {
         uint2 r[U];
@@ -2181,13 +2181,22 @@ uint64_t initial_chunk(const Workspace& ws, uint64_t n) {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         const double per_slot = kCandSlotBytes;
-        const double afford = 0.75 * static_cast<double>(free_b) / per_slot + static_cast<double>(ws.cand_cap);
+        const double afford = std::min(0.75 * static_cast<double>(free_b) / per_slot + static_cast<double>(ws.cand_cap),
+                                       static_cast<double>(kMaxCandSlots));
         const double fit = afford / (ws.cand_density * 1.1);
         if (fit < static_cast<double>(c)) c = std::max<uint64_t>(static_cast<uint64_t>(fit), 1);
     }
     return c;
 }
 
+// The next chunk of the `left` guides still to score when a run may take at most `most`: the
+// remainder cut into equal pieces (chunks of a split call take about the same time and memory, and
+// no small last chunk streams the lists for a handful of guides).
+uint64_t balanced_chunk(uint64_t most, uint64_t left) {
+    most = std::max<uint64_t>(most, 1);
+    const uint64_t pieces = (left + most - 1) / most;
+    return (left + pieces - 1) / pieces;
+}
 
 // Scores the guides in one run, or, when the device cannot hold the workspace a run needs (the
 // candidates of many promiscuous guides), in consecutive chunks of guides, halving the chunk
@@ -2199,7 +2208,7 @@ void run_scoring(issl_index* ix, const uint64_t* d_qsig_in, uint64_t n, const Sc
     issl_score_stats sum{};
     uint64_t chunk = initial_chunk(ws, n), done = 0;
     while (done < n) {
-        const uint64_t k = std::min(chunk, n - done);
+        const uint64_t k = balanced_chunk(chunk, n - done);
         RunSpec R;
         R.qsig = d_qsig_in + done;
         R.n = k;
@@ -2337,7 +2346,7 @@ void run_batch_chunked(issl_batch* b, uint64_t n, const issl_guide_set* sets, si
     issl_score_stats sum{};
     uint64_t chunk = initial_chunk(ws, n), done = 0;
     while (done < n) {
-        const uint64_t k = std::min(chunk, n - done);
+        const uint64_t k = balanced_chunk(chunk, n - done);
         std::vector<issl_guide_set> sub;  // the sets, cut to [done, done + k)
         uint64_t pos = 0;
         for (size_t i = 0; i < n_sets; i++) {
