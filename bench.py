@@ -733,7 +733,8 @@ def bench_capacity(args, pkg):
         "config": dict(CAPACITY, n_sites=n_sites, n_queries=nq, entry_bytes=info.entry_bytes,
                        resident_gb=info.device_bytes / 1e9, generation_s=gen_s),
         "stats": {"scan_ms": st.scan_ms, "scan_bytes": st.scan_bytes, "hits": st.hits, "candidates": st.candidates,
-                  "probes": st.probes, "launches": st.launches, "dropped_hits": st.dropped_hits},
+                  "probes": st.probes, "launches": st.launches, "dropped_hits": st.dropped_hits,
+                  "pipeline_runs": st.runs},
         "tuning": tuning, "parity_sample": parity, "clocks": clocks.summary(),
     }
 

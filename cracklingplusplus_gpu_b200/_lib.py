@@ -37,7 +37,7 @@ class ScoreStats(C.Structure):
                 ("buckets_scanned", C.c_uint64), ("entries_scanned", C.c_uint64), ("units", C.c_uint64),
                 ("hits", C.c_uint64), ("scan_bytes", C.c_uint64), ("launches", C.c_uint64),
                 ("class_probes", C.c_uint64 * 3), ("candidates", C.c_uint64), ("staged_bytes", C.c_uint64),
-                ("dropped_hits", C.c_uint64), ("replayed", C.c_uint64)]
+                ("dropped_hits", C.c_uint64), ("replayed", C.c_uint64), ("runs", C.c_uint64)]
 
 
 class Tuning(C.Structure):

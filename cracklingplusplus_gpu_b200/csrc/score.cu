@@ -5,9 +5,10 @@
 // run once per slice wave (the first slices, then the rest) for the guides still scoring:
 //   1 probe_count   every (guide, wave slice) pair -> its global bucket; count probes per bucket
 //   2 bucket scan   exclusive scan over the wave's buckets of (scan units, probes): per-bucket
-//                   probe slot ranges, and unit descriptors -- a unit is (bucket chunk of up to
-//                   kChunk entries) x (up to kGroup guides probing that bucket), so guides sharing
-//                   a bucket read its entries once and heavy buckets split into many units
+//                   probe slot ranges, and unit descriptors -- a unit is (up to 32 consecutive
+//                   32-entry blocks of a bucket) x (up to kGroup guides probing that bucket), so
+//                   guides sharing a bucket read its entries once and heavy buckets split into
+//                   many units
 //   3 probe_scatter guides grouped by bucket, with each guide's residual code for that slice
 //   4 scan          persistent, work-stealing: stream the bit-sliced residual codes of every unit
 //                   through per-warp bulk-copy rings; a candidate is an entry whose residual
@@ -124,7 +125,6 @@ constexpr uint32_t kCandSlab = 256;
 // candidate slots of one wave are addressed with 32 bits: the capacity stays below this
 constexpr size_t kMaxCandSlots = 0xFFFFFFFFull - (1ull << 20);
 constexpr uint32_t kDeadCand = 0xFFFFFFFFu;  // guide field of an unused or rejected candidate slot
-constexpr uint32_t kNoSite = 0xFFFFFFFFu;  // grouped-hit id of a record that counts for nothing
 constexpr int kGuideBits = 26;               // candidate records pack guide | slice << 26
 constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 1.965 GHz
 
@@ -224,7 +224,7 @@ struct issl::Workspace {
     uint32_t graph_tuning = ~0u;
     uint64_t graph_kernels = 0;
     // host-list index: two device windows of staged slices, the stream that fills them, and the
-    // events that order the fills with the scans (window b is free again once the hit scatter of
+    // events that order the fills with the scans (window b is free again once the resolve pass of
     // the wave that used it has run)
     DevBuf<uint32_t> win_ids[2], win_rbits[2];
     cudaStream_t copy_stream = nullptr;
@@ -833,7 +833,7 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
 // MIT and CFD contributions are computed here, where the reads leave the arithmetic units idle, and
 // its record is written to the next free slot of its guide's segment, so the scorers read only
 // contiguous data.
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 5)
     k_cand_resolve(const uint2* __restrict__ cands, Counters* c, IndexView ix, const uint64_t* __restrict__ qsig,
                    const uint32_t* __restrict__ qoff, uint32_t* __restrict__ qfill, const Tables* __restrict__ tables,
                    HitRec* __restrict__ seg, const SetDesc* __restrict__ sets, const uint16_t* __restrict__ qset) {
@@ -854,9 +854,9 @@ __global__ void __launch_bounds__(256, 4)
     both.calc_cfd = 1;
     const uint32_t n = c->n_cand;
     uint32_t owned_here = 0;
-    // four candidates per thread and round, their reads issued together (the random list-entry
-    // reads are the bound: more of them in flight per thread)
-    constexpr int U = 4;
+    // two candidates per thread and round, their reads issued together (the random list-entry
+    // reads are the bound: more of them in flight per thread; four gave no further gain)
+    constexpr int U = 2;
     const uint32_t T = gridDim.x * blockDim.x;
     for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * T) {
         uint2 r[U];
@@ -1142,7 +1142,7 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         if (P.want_distinct)
             for (uint32_t j = lane; j < L; j += 32) {
                 const uint32_t id = seg[j].r.z;
-                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
         if (lane == 0) {
             if (a.last_wave) {
@@ -1309,11 +1309,11 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
         if (P.want_distinct) {  // the sites of the slices before the exit slice, then up to the stop
             for (uint32_t j = lane; j < b0; j += 32) {
                 const uint32_t id = seg[W.idx[j]].r.z;
-                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
             for (uint32_t j = lane; j <= stop; j += 32) {
                 const uint32_t id = seg[W.keys[j] & 1023u].r.z;
-                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
         }
         if (lane == 0) finalise(P, dm, dc, rn, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
@@ -1442,7 +1442,7 @@ __global__ void __launch_bounds__(256) k_score_block(ScoreArgs a) {
             for (uint32_t t = threadIdx.x; t <= stop; t += blockDim.x) {
                 const uint32_t h = in_smem ? static_cast<uint32_t>(s_bkeys[t] & ((1u << kBlockIdxBits) - 1)) : t;
                 const uint32_t id = seg[h].r.z;
-                if (id != kNoSite) atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
+                atomicOr(&a.bitmap[id >> 5], 1u << (id & 31));
             }
         if (threadIdx.x == 0) finalise(P, dm, dc, run_n, qi, a.out_mit, a.out_cfd, a.out_code, a.out_count);
         __syncthreads();
@@ -1910,7 +1910,7 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         const int wb = static_cast<int>(w & 1u);  // device window of this wave (host-list index)
         if (staged) {
             // stage the wave's slices: entries and bit-sliced codes, on the copy stream, once the
-            // window is free (its previous wave's hit scatter has run)
+            // window is free (its previous wave's resolve pass has run)
             const uint64_t N = ix->n_sites, ew = ix->entry_words;
             uint64_t wbase0, words;
             window_rbits(ix, s0, s1, &wbase0, &words);
@@ -2093,6 +2093,7 @@ void fill_stats(const Workspace& ws, float scan_ms, float total_ms, uint64_t lau
     s.staged_bytes = ws.staged;
     s.dropped_hits = ws.last.dropped;
     s.replayed = ws.last.n_replay;
+    s.runs = 1;
 }
 
 issl_score_stats run_stats(issl_index* ix, Workspace& ws) {
@@ -2125,6 +2126,7 @@ void add_stats(issl_score_stats& a, const issl_score_stats& b) {
     a.staged_bytes += b.staged_bytes;
     a.dropped_hits += b.dropped_hits;
     a.replayed += b.replayed;
+    a.runs += b.runs;
 }
 
 // One pipeline run over n guides, growing the workspace and rerunning on overflow.
@@ -2136,7 +2138,11 @@ issl_score_stats run_once(issl_index* ix, Workspace& ws, RunSpec R, uint64_t* d_
             k_copy_distinct<<<1, 1, 0, st>>>(ws.counters.p, d_distinct);
             ws.launches++;
         }
-        if (check_and_grow(ws, st)) return run_stats(ix, ws);
+        if (check_and_grow(ws, st)) {
+            issl_score_stats s = run_stats(ix, ws);
+            s.runs = attempt + 1;  // with the runs that overflowed and were repeated
+            return s;
+        }
     }
     throw Error(ISSL_ERR_NOMEM, "scoring workspace kept overflowing");
 }
@@ -2152,13 +2158,18 @@ void learn_density(Workspace& ws, uint64_t k, double cands) {
 void learn_density(Workspace& ws, uint64_t k) { learn_density(ws, k, static_cast<double>(ws.last.max_cand)); }
 
 // After a run of k guides that needed more candidate slots than the device can hold: the chunk
-// of guides whose candidates fit in about 3/4 of the free memory, at the demand the failed run
-// measured (its candidate counter keeps counting past the buffer), never more than half of k.
+// of guides whose candidates fit in the buffers held plus about 3/4 of the free memory, at the
+// demand the failed run measured (its candidate counter keeps counting past the buffer), never
+// more than half of k.
 uint64_t shrunk_chunk(Workspace& ws, uint64_t k) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     const double per_slot = kCandSlotBytes;
-    const double afford = 0.75 * static_cast<double>(free_b) / per_slot;
+    // the candidate and hit buffers the workspace already holds count as affordable too (a failed
+    // growth leaves them allocated, so the free memory alone would shrink the chunk too far)
+    const double held = static_cast<double>(ws.cands.bytes() + ws.seg.bytes());
+    const double afford = std::min((0.75 * static_cast<double>(free_b) + held) / per_slot,
+                                   static_cast<double>(kMaxCandSlots));
     const double demand = static_cast<double>(std::max<uint64_t>(ws.last.max_cand, 1));
     learn_density(ws, k, demand);  // size the next run from what this one needed
     uint64_t c = static_cast<uint64_t>(static_cast<double>(k) * std::min(0.5, afford / demand));
@@ -2181,7 +2192,8 @@ uint64_t initial_chunk(const Workspace& ws, uint64_t n) {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         const double per_slot = kCandSlotBytes;
-        const double afford = std::min(0.75 * static_cast<double>(free_b) / per_slot + static_cast<double>(ws.cand_cap),
+        const double held = static_cast<double>(ws.cands.bytes() + ws.seg.bytes());
+        const double afford = std::min((0.75 * static_cast<double>(free_b) + held) / per_slot,
                                        static_cast<double>(kMaxCandSlots));
         const double fit = afford / (ws.cand_density * 1.1);
         if (fit < static_cast<double>(c)) c = std::max<uint64_t>(static_cast<uint64_t>(fit), 1);
@@ -2330,6 +2342,7 @@ void run_batch(issl_batch* b, uint64_t n, const issl_guide_set* sets, size_t n_s
             float total = 0.f;
             cudaEventElapsedTime(&total, b->ev0, b->ev1);
             fill_stats(ws, 0.f, total, ws.graph_kernels, b->stats);
+            b->stats.runs = attempt + 1;
             return;
         }
     }

@@ -180,6 +180,8 @@ typedef struct {
                                    ISSL_ERR_INTERNAL */
     uint64_t replayed;          /* guides whose decision lay within the reference's rounding of
                                    its running sums, rescored one addition at a time */
+    uint64_t runs;              /* pipeline runs of the call: one per guide chunk, plus any run
+                                   repeated after its buffers had to grow */
 } issl_score_stats;
 
 /* Frees the device memory of the index's own scoring workspace (the buffers the plain
