@@ -647,6 +647,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
     uint4 dA = take_batch(), dB = make_uint4(0, 0, 0, 0);
     bool have_b = false;
     uint32_t issued = 0;  // units of this warp issued so far (unit t lives in ring stage t % NS)
+    uint32_t ist = 0;     // ring stage of the next unit to issue (issued % NS, kept without a divide)
     uint32_t slot = 0;    // slot of the next unit in batch A
     bool ended = false;
 
@@ -671,7 +672,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
         }
         const uint32_t p0 = __shfl_sync(0xffffffffu, dA.x, slot), qbeg = __shfl_sync(0xffffffffu, dA.y, slot);
         if (lane == 0) {
-            const uint32_t st = issued % NS;
+            const uint32_t st = ist;
             const uint32_t len = dz & 0xFFFFu, qn = (dz >> 16) & 0xFFu, s = dz >> 24;
             const uint32_t b0 = p0 / 32u, nb = (p0 + len - 1) / 32u - b0 + 1;  // <= 32: inside one chunk
             const uint32_t wpb = sh.wpb[s];
@@ -698,6 +699,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
         }
         slot++;
         issued++;
+        if (++ist == NS) ist = 0;
     };
 
     ScanCtx cx{0u, 0u, false};
