@@ -122,6 +122,7 @@ __device__ __forceinline__ uint64_t chunk_of(uint64_t bucket_size, const ChunkCl
 constexpr int kMaxStages = 4;
 constexpr int kStageQr = kGroup + 2;     // (guide, residual) pairs per stage + alignment slack
 constexpr uint32_t kCandSlab = 256;
+constexpr uint32_t kScanRecs = 64;  // per-warp buffer of candidate records (guide, lane, word)
 // candidate slots of one wave are addressed with 32 bits: the capacity stays below this
 constexpr size_t kMaxCandSlots = 0xFFFFFFFFull - (1ull << 20);
 constexpr uint32_t kDeadCand = 0xFFFFFFFFu;  // guide field of an unused or rejected candidate slot
@@ -143,7 +144,7 @@ struct StageMeta {
 struct WarpLayout {
     uint32_t stages;
     uint32_t stage_words;  // 32 blocks x words per block (largest slice)
-    uint32_t qr_off, qm_off, meta_off, bar_off, bytes;
+    uint32_t qr_off, qm_off, rec_off, meta_off, bar_off, bytes;
 };
 
 __host__ __device__ inline WarpLayout warp_layout(uint32_t max_wpb, uint32_t stages) {
@@ -152,7 +153,8 @@ __host__ __device__ inline WarpLayout warp_layout(uint32_t max_wpb, uint32_t sta
     L.stage_words = (32u * max_wpb + 3u + 3u) & ~3u;  // 32 blocks + alignment slack, 16-byte multiple
     L.qr_off = stages * L.stage_words * 4u;                 // 16-byte aligned (stage_words % 4 == 0)
     L.qm_off = L.qr_off + stages * kStageQr * 8u;
-    L.meta_off = L.qm_off + 64u * 4u;  // two 32-word guide-mask buffers
+    L.rec_off = L.qm_off + 64u * 4u;  // two 32-word guide-mask buffers
+    L.meta_off = L.rec_off + kScanRecs * 8u;
     L.bar_off = L.meta_off + stages * static_cast<uint32_t>(sizeof(StageMeta));
     L.bytes = (L.bar_off + stages * 8u + 15u) & ~15u;
     return L;
@@ -521,13 +523,65 @@ struct ScanCtx {  // per-warp state of the candidate slab
     bool full;
 };
 
+// Writes the warp's candidate records out: record r is (guide | lane << 26, word), the entries of
+// block b0 + lane within the bound for that guide. Every lane takes one record per round; the
+// round's candidates are counted per guide and written as (guide | slice << 26, list position) to
+// consecutive slots of the warp's slab (k_cand_resolve then reads each one's list entry and applies
+// the ownership rule to the site's mismatch positions).
+__device__ __forceinline__ void flush_records(const ScanArgs& a, const uint2* rec, uint32_t nrec, const StageMeta& m,
+                                              int lane, ScanCtx& cx) {
+    __syncwarp();  // the records are written
+    for (uint32_t r0 = 0; r0 < nrec; r0 += 32) {
+        const uint32_t j = r0 + static_cast<uint32_t>(lane);
+        const uint2 rc = j < nrec ? rec[j] : make_uint2(0u, 0u);
+        const uint32_t c = __popc(rc.y);
+        uint32_t inc = c;  // inclusive prefix over the lanes
+#pragma unroll
+        for (int dd = 1; dd < 32; dd <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, inc, dd);
+            if (lane >= dd) inc += o;
+        }
+        const uint32_t tot = __shfl_sync(0xffffffffu, inc, 31);
+        if (cx.cpos + tot > cx.cend) {
+            // retire the rest of the slab, reserve a new one (at least the round's candidates)
+            for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
+                if (i < a.cand_cap) a.cands[i] = make_uint2(kDeadCand, 0);
+            // 64-bit reservations: a wave may ask for more than 2^32 slots (the host then splits
+            // the guides); a slab past the capacity is never written
+            const uint32_t want = tot > kCandSlab ? tot : kCandSlab;
+            uint32_t base = 0, full = 0;
+            if (lane == 0) {
+                const unsigned long long b = atomicAdd(&a.counters->cand_reserved, static_cast<unsigned long long>(want));
+                full = b + want > a.cand_cap;
+                base = full ? a.cand_cap : static_cast<uint32_t>(b);
+            }
+            cx.cpos = __shfl_sync(0xffffffffu, base, 0);
+            cx.cend = cx.cpos + want;
+            cx.full = __shfl_sync(0xffffffffu, full, 0) != 0;
+        }
+        if (c) {
+            const uint32_t g = rc.x & ((1u << kGuideBits) - 1u);
+            atomicAdd(&a.qcand[g], c);
+            if (!cx.full) {
+                const uint32_t gx = g | (m.s << kGuideBits), p = 32u * (m.b0 + (rc.x >> kGuideBits));
+                uint32_t o = cx.cpos + inc - c;
+                for (uint32_t bits = rc.y; bits; bits &= bits - 1u) a.cands[o++] = make_uint2(gx, p + __ffs(bits) - 1u);
+            }
+        }
+        cx.cpos += tot;
+    }
+    __syncwarp();  // the record buffer is read
+}
+
 // Compares every guide of the unit with the lane's block (RW residual positions per entry).
 template <int RW>
 __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb, const uint64_t* qr, uint32_t* qm,
-                                          const StageMeta& m, uint32_t wpb, int lane, int max_dist, ScanCtx& cx) {
+                                          uint2* rec, const StageMeta& m, uint32_t wpb, int lane, int max_dist,
+                                          ScanCtx& cx) {
     constexpr int NW = 2 * RW;
     constexpr int NV = (NW + 3) / 4;
     const unsigned lt = (1u << lane) - 1u;
+    uint32_t nrec = 0;  // candidate records of the unit not yet written out (uniform)
     // this lane's block and the entries of it that belong to the unit (unsigned arithmetic: list
     // positions reach 2^32 - 1; the unit starts in block b0 and ends after this lane's block start)
     uint32_t d[NW];
@@ -570,46 +624,30 @@ __device__ __forceinline__ void scan_unit(const ScanArgs& a, const uint32_t* rb,
             if (2 * v < RW) mm[2 * v] = (d[4 * v] ^ w.x) | (d[4 * v + 1] ^ w.y);
             if (2 * v + 1 < RW) mm[2 * v + 1] = (d[4 * v + 2] ^ w.z) | (d[4 * v + 3] ^ w.w);
         }
-        uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), max_dist) & valid;
-        // candidates are rare: one per lane per round, written to the warp's slab as (guide |
-        // slice << 26, list position) and counted per guide; k_cand_resolve reads each one's list
-        // entry and applies the ownership rule to the site's mismatch positions
-        const uint32_t gx = static_cast<uint32_t>(g) | (m.s << kGuideBits);
-        for (unsigned hm = __ballot_sync(0xffffffffu, cbits != 0); hm; hm = __ballot_sync(0xffffffffu, cbits != 0)) {
-            const uint32_t nh = __popc(hm);
-            if (lane == 0) atomicAdd(&a.qcand[static_cast<uint32_t>(g)], nh);
-            if (cx.cpos + nh > cx.cend) {
-                // retire the rest of the slab, reserve a new one
-                for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
-                    if (i < a.cand_cap) a.cands[i] = make_uint2(kDeadCand, 0);
-                // 64-bit reservations: a wave may ask for more than 2^32 slots (the host then splits
-                // the guides); a slab past the capacity is never written
-                uint32_t base = 0, full = 0;
-                if (lane == 0) {
-                    const unsigned long long b = atomicAdd(&a.counters->cand_reserved, static_cast<unsigned long long>(kCandSlab));
-                    full = b + kCandSlab > a.cand_cap;
-                    base = full ? a.cand_cap : static_cast<uint32_t>(b);
-                }
-                cx.cpos = __shfl_sync(0xffffffffu, base, 0);
-                cx.cend = cx.cpos + kCandSlab;
-                cx.full = __shfl_sync(0xffffffffu, full, 0) != 0;
-            }
-            if (cbits) {
-                const int e = __ffs(cbits) - 1;
-                cbits &= cbits - 1;
-                if (!cx.full) a.cands[cx.cpos + __popc(hm & lt)] = make_uint2(gx, 32u * bl + e);
-            }
-            cx.cpos += nh;
+        const uint32_t cbits = bs::within(bs::count_mismatches<RW>(mm), max_dist) & valid;
+        // candidate words are rare (about two lanes per guide and unit): each lane with one
+        // appends (guide | lane << 26, word) to the warp's record buffer, which is written out
+        // when it may not take another guide's 32 and when the unit ends. The comparison loop
+        // itself has no branch on the data.
+        const unsigned hm = __ballot_sync(0xffffffffu, cbits != 0);
+        if (nrec > kScanRecs - 32u) {
+            flush_records(a, rec, nrec, m, lane, cx);
+            nrec = 0;
         }
+        if (cbits)
+            rec[nrec + __popc(hm & lt)] = make_uint2(static_cast<uint32_t>(g) | (static_cast<uint32_t>(lane) << kGuideBits), cbits);
+        nrec += __popc(hm);
     }
+    if (nrec) flush_records(a, rec, nrec, m, lane, cx);
 }
 
 // RWFIX > 0: every slice of the index has RWFIX residual positions; 0: mixed widths.
 // Persistent and work-stealing: each warp takes batches of 32 consecutive units from a global
 // queue (one atomic per batch), so warps that draw heavy units (hot repeat buckets with a full
-// group of guides) simply take fewer batches.
+// group of guides) simply take fewer batches. The 10- and 12-position scans keep to 72 registers,
+// so that seven blocks fit an SM (the shared-memory limit at two stages); the others to 96 (five).
 template <int RWFIX>
-__global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
+__global__ void __launch_bounds__(kScanWarps * 32, RWFIX == 12 || RWFIX == 10 ? 7 : 5) k_scan(ScanArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     __shared__ ScanShared sh;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -619,6 +657,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
     uint32_t* rb = reinterpret_cast<uint32_t*>(wbase_ptr);
     uint64_t* qr = reinterpret_cast<uint64_t*>(wbase_ptr + L.qr_off);
     uint32_t* qm = reinterpret_cast<uint32_t*>(wbase_ptr + L.qm_off);
+    uint2* rec = reinterpret_cast<uint2*>(wbase_ptr + L.rec_off);
     StageMeta* meta = reinterpret_cast<StageMeta*>(wbase_ptr + L.meta_off);
     uint64_t* bar = reinterpret_cast<uint64_t*>(wbase_ptr + L.bar_off);
     for (int i = threadIdx.x; i < static_cast<int>(a.n_slices); i += blockDim.x) {
@@ -719,18 +758,18 @@ __global__ void __launch_bounds__(kScanWarps * 32) k_scan(ScanArgs a) {
         const uint32_t* srb = rb + st * L.stage_words;
         const uint64_t* sqr = qr + st * kStageQr;
         if constexpr (RWFIX > 0) {
-            scan_unit<RWFIX>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx);
+            scan_unit<RWFIX>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx);
         } else switch (sh.rw[m.s]) {  // uniform across the warp
-            case 12: scan_unit<12>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
-            case 10: scan_unit<10>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
-            case 16: scan_unit<16>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
-            case 15: scan_unit<15>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
-            case 14: scan_unit<14>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
-            case 13: scan_unit<13>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
-            case 11: scan_unit<11>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
-            case 9: scan_unit<9>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
-            case 8: scan_unit<8>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
-            default: scan_unit<7>(a, srb, sqr, qm, m, wpb, lane, max_dist, cx); break;
+            case 12: scan_unit<12>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
+            case 10: scan_unit<10>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
+            case 16: scan_unit<16>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
+            case 15: scan_unit<15>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
+            case 14: scan_unit<14>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
+            case 13: scan_unit<13>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
+            case 11: scan_unit<11>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
+            case 9: scan_unit<9>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
+            case 8: scan_unit<8>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
+            default: scan_unit<7>(a, srb, sqr, qm, rec, m, wpb, lane, max_dist, cx); break;
         }
         __syncwarp();  // every lane is done with stage st before it is refilled
         try_issue();
