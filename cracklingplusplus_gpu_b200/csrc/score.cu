@@ -347,98 +347,98 @@ __device__ __forceinline__ uint64_t slice_of_entry(uint64_t e, uint64_t n, doubl
     return s;
 }
 
-// Unit descriptors, up to kUnitsPerThread consecutive units per thread (one when the units are too
-// few to give every thread of the grid several). The first unit's bucket is the
-// last bucket of the wave whose first unit is at or before it (binary search of the units'
-// exclusive prefix; empty buckets share their successor's prefix, so the search lands on the
-// bucket that owns the unit). The following units stay in that bucket or gallop forward to theirs
-// (a walk one bucket at a time would crawl over the empty buckets of sparse waves). A bucket's
-// units run over the chunk-aligned blocks of its list range, and within a block over its groups
-// of up to kGroup guides.
-constexpr uint32_t kUnitsPerThread = 8;
-__global__ void k_expand_units(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off,
-                               const uint32_t* __restrict__ qstart, const uint32_t* __restrict__ ustart, uint64_t g0,
-                               uint64_t nb, uint64_t n_sites, double inv_n, ChunkClasses cc,
-                               const Counters* __restrict__ ctr, UnitDesc* __restrict__ units) {
-    const uint32_t n = ctr->n_units;  // at most the buffer's capacity
-    const uint64_t g_end = g0 + nb;
-    const uint64_t threads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    const uint64_t upt = std::min<uint64_t>(kUnitsPerThread, std::max<uint64_t>(1, (n + threads - 1) / threads));
-    for (uint64_t base = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) * upt; base < n;
-         base += threads * upt) {
-        uint64_t lo = 0, hi = nb;  // first bucket whose first unit is after `base`
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (ustart[g0 + mid] <= base) lo = mid + 1;
-            else hi = mid;
-        }
-        uint64_t g = g0 + lo - 1, have = ~0ull;
-        uint32_t c = 0, u0 = 0, lc = 0, ng = 1, q0 = 0;
-        uint64_t s = 0, e0 = 0, e1 = 0;
-        const uint64_t last = base + upt < n ? base + upt : n;
-        for (uint64_t u = base; u < last; u++) {
-            if (g + 1 < g_end && ustart[g + 1] <= u) {  // u is in a later bucket: gallop, then bisect
-                uint64_t a = g + 1, b = a + 1, step = 1;  // ustart[a] <= u
-                while (b < g_end && ustart[b] <= u) {
-                    a = b;
-                    step <<= 1;
-                    b = a + step;
-                }
-                if (b > g_end) b = g_end;  // b == g_end or ustart[b] > u
-                while (b - a > 1) {
-                    const uint64_t mid = (a + b) >> 1;
-                    if (ustart[mid] <= u) a = mid;
-                    else b = mid;
-                }
-                g = a;
-            }
-            if (g != have) {
-                have = g;
-                c = cnt[g];
-                u0 = ustart[g];
-                q0 = qstart[g];
-                s = slice_of_entry(off[g], n_sites, inv_n);
-                e0 = off[g] - s * n_sites;  // list positions
-                e1 = off[g + 1] - s * n_sites;
-                lc = __ffs(static_cast<uint32_t>(chunk_of(e1 - e0, cc))) - 1;  // unit sizes are powers of 2
-                ng = (c + kGroup - 1) / kGroup;
-            }
-            const uint32_t r = static_cast<uint32_t>(u) - u0;
-            const uint32_t k = r / ng, j = r - k * ng;
-            // unit k: blocks [B0 + k * C/32, B0 + (k + 1) * C/32) of the bucket, B0 its first block
-            const uint64_t B0 = e0 >> 5;
-            const uint64_t first = (B0 + (static_cast<uint64_t>(k) << (lc - 5))) << 5;
-            const uint64_t last = (B0 + (static_cast<uint64_t>(k + 1) << (lc - 5))) << 5;
-            const uint64_t cb = first > e0 ? first : e0;
-            const uint64_t ce = last < e1 ? last : e1;
-            UnitDesc d;
-            d.p0 = static_cast<uint32_t>(cb);
-            d.qbeg = q0 + j * kGroup;
-            d.len = static_cast<uint16_t>(ce - cb);
-            d.qn = static_cast<uint8_t>(c - j * kGroup < kGroup ? c - j * kGroup : kGroup);
-            d.s = static_cast<uint8_t>(s);
-            d.pad = 0;
-            units[u] = d;
-        }
-    }
+// Unit descriptors. A bucket's units run over the chunk-aligned blocks of its list range (counted
+// from its first block), and within a chunk over its groups of up to kGroup guides: unit r of the
+// bucket is chunk r / groups, group r % groups, and lands at ustart[bucket] + r. Each lane reads
+// one bucket; the units of the warp's 32 buckets are consecutive and the warp writes them 32 at a
+// time, so hot buckets probed by many guides spread over the lanes too. The same pass adds up the
+// wave's work counters for the roofline:
+// distinct buckets scanned, entries compared and bit-sliced bytes copied (once per guide group),
+// and the probes per bucket-size class.
+struct UnitSpan {
+    uint64_t e0, e1;   // list range of the bucket
+    uint32_t c;        // guides probing it
+    uint32_t ng, lc;   // guide groups, log2 of the unit size
+    uint32_t u0, q0;   // first unit, first probe slot
+    uint32_t s;        // slice
+};
+__device__ __forceinline__ void write_unit(const UnitSpan& b, uint32_t r, uint32_t n, UnitDesc* __restrict__ units) {
+    const uint32_t u = b.u0 + r;
+    if (u >= n) return;  // past the buffer's capacity: the host grows it and reruns
+    const uint32_t k = r / b.ng, j = r - k * b.ng;
+    const uint64_t B0 = b.e0 >> 5;
+    const uint64_t first = (B0 + (static_cast<uint64_t>(k) << (b.lc - 5))) << 5;
+    const uint64_t last = (B0 + (static_cast<uint64_t>(k + 1) << (b.lc - 5))) << 5;
+    const uint64_t cb = first > b.e0 ? first : b.e0;
+    const uint64_t ce = last < b.e1 ? last : b.e1;
+    UnitDesc d;
+    d.p0 = static_cast<uint32_t>(cb);
+    d.qbeg = b.q0 + j * kGroup;
+    d.len = static_cast<uint16_t>(ce - cb);
+    d.qn = static_cast<uint8_t>(b.c - j * kGroup < kGroup ? b.c - j * kGroup : kGroup);
+    d.s = static_cast<uint8_t>(b.s);
+    d.pad = 0;
+    units[u] = d;
 }
 
-// work counters for the roofline: distinct buckets scanned and entries streamed (a bucket's
-// entries are read once per group of up to kGroup guides)
-__global__ void k_bucket_stats(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off, uint64_t g0,
-                               uint64_t g1, const SliceGeom* __restrict__ geom, uint64_t n_sites, Counters* c) {
+__global__ void k_expand_units(const uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off,
+                               const uint32_t* __restrict__ qstart, const uint32_t* __restrict__ ustart, uint64_t g0,
+                               uint64_t g1, uint64_t n_sites, double inv_n, ChunkClasses cc,
+                               const SliceGeom* __restrict__ geom, Counters* __restrict__ ctr,
+                               UnitDesc* __restrict__ units) {
+    const uint32_t n = ctr->n_units;  // at most the buffer's capacity
+    const int lane = threadIdx.x & 31;
     uint64_t buckets = 0, entries = 0, bytes = 0, cp[3] = {0, 0, 0};
-    for (uint64_t g = g0 + blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < g1;
-         g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t k = cnt[g];
-        if (!k) continue;
-        const uint64_t groups = (k + kGroup - 1) / kGroup;
-        const uint64_t s = off[g] / n_sites, p0 = off[g] - s * n_sites, p1 = off[g + 1] - s * n_sites;
-        buckets++;
-        entries += (p1 - p0) * groups;
-        // bit-sliced blocks copied: every block the bucket touches, once per guide group
-        bytes += ((p1 - 1) / 32 - p0 / 32 + 1) * geom[s].wpb * 4ull * groups;
-        cp[(p1 - p0) < 64 ? 0 : (p1 - p0) < 4096 ? 1 : 2] += k;
+    // warp-aligned grid stride, so that the hot-bucket path below is uniform across the warp
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = g0 + blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g - lane < g1; g += stride) {
+        UnitSpan b{0, 0, 0, 1, 5, 0, 0, 0};
+        uint32_t nu = 0, u0 = 0xFFFFFFFFu;  // past the wave: after every unit
+        if (g < g1) {
+            b.c = cnt[g];
+            u0 = ustart[g];
+        }
+        if (b.c) {
+            b.s = static_cast<uint32_t>(slice_of_entry(off[g], n_sites, inv_n));
+            b.e0 = off[g] - b.s * n_sites;  // list positions
+            b.e1 = off[g + 1] - b.s * n_sites;
+            const uint64_t C = chunk_of(b.e1 - b.e0, cc);
+            b.lc = __ffs(static_cast<uint32_t>(C)) - 1;  // unit sizes are powers of 2
+            b.ng = (b.c + kGroup - 1) / kGroup;
+            b.u0 = u0;
+            b.q0 = qstart[g];
+            const uint64_t nb = ((b.e1 - 1) >> 5) - (b.e0 >> 5) + 1;  // blocks the bucket touches
+            nu = static_cast<uint32_t>((nb - 1) / (C >> 5) + 1) * b.ng;
+            buckets++;
+            entries += (b.e1 - b.e0) * b.ng;
+            bytes += nb * geom[b.s].wpb * 4ull * b.ng;
+            const uint64_t len = b.e1 - b.e0;
+            cp[0] += len < 64 ? b.c : 0u;
+            cp[1] += len >= 64 && len < 4096 ? b.c : 0u;
+            cp[2] += len >= 4096 ? b.c : 0u;
+        }
+        // the warp's buckets own the consecutive units [U0, U0 + T); each round lane l writes unit
+        // U0 + t0 + l (coalesced), whose bucket is that of the last lane starting at or before it
+        // (an empty bucket starts where the next non-empty one does, so that lane is non-empty)
+        const uint32_t T = __reduce_add_sync(0xffffffffu, nu);
+        const uint32_t U0 = __shfl_sync(0xffffffffu, u0, 0);
+        for (uint32_t t0 = 0; t0 < T; t0 += 32) {
+            const uint32_t w = U0 + t0 + static_cast<uint32_t>(lane);
+            int o = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+                if (__shfl_sync(0xffffffffu, u0, o + step) <= w) o += step;
+            UnitSpan h;
+            h.e0 = __shfl_sync(0xffffffffu, b.e0, o);
+            h.e1 = __shfl_sync(0xffffffffu, b.e1, o);
+            h.c = __shfl_sync(0xffffffffu, b.c, o);
+            h.ng = __shfl_sync(0xffffffffu, b.ng, o);
+            h.lc = __shfl_sync(0xffffffffu, b.lc, o);
+            h.u0 = __shfl_sync(0xffffffffu, u0, o);
+            h.q0 = __shfl_sync(0xffffffffu, b.q0, o);
+            h.s = __shfl_sync(0xffffffffu, b.s, o);
+            if (t0 + lane < T) write_unit(h, w - h.u0, n, units);
+        }
     }
     for (int d = 16; d > 0; d >>= 1) {
         buckets += __shfl_down_sync(0xffffffffu, buckets, d);
@@ -446,12 +446,12 @@ __global__ void k_bucket_stats(const uint32_t* __restrict__ cnt, const uint64_t*
         bytes += __shfl_down_sync(0xffffffffu, bytes, d);
         for (int i = 0; i < 3; i++) cp[i] += __shfl_down_sync(0xffffffffu, cp[i], d);
     }
-    if ((threadIdx.x & 31) == 0 && buckets) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(&c->buckets), buckets);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&c->entries), entries);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&c->rbytes), bytes);
+    if (lane == 0 && buckets) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->buckets), buckets);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->entries), entries);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->rbytes), bytes);
         for (int i = 0; i < 3; i++)
-            if (cp[i]) atomicAdd(reinterpret_cast<unsigned long long*>(&c->class_probes[i]), cp[i]);
+            if (cp[i]) atomicAdd(reinterpret_cast<unsigned long long*>(&ctr->class_probes[i]), cp[i]);
     }
 }
 
@@ -535,13 +535,19 @@ __device__ __forceinline__ void flush_records(const ScanArgs& a, const uint2* re
         const uint32_t j = r0 + static_cast<uint32_t>(lane);
         const uint2 rc = j < nrec ? rec[j] : make_uint2(0u, 0u);
         const uint32_t c = __popc(rc.y);
-        uint32_t inc = c;  // inclusive prefix over the lanes
+        // slot of the lane's first candidate within the round: usually every record holds one
+        // candidate and the lane's own index is its offset; otherwise an inclusive prefix
+        uint32_t inc = j < nrec ? static_cast<uint32_t>(lane) + 1u : 0u;
+        uint32_t tot = nrec - r0 < 32u ? nrec - r0 : 32u;
+        if (__ballot_sync(0xffffffffu, c > 1u)) {
+            inc = c;
 #pragma unroll
-        for (int dd = 1; dd < 32; dd <<= 1) {
-            const uint32_t o = __shfl_up_sync(0xffffffffu, inc, dd);
-            if (lane >= dd) inc += o;
+            for (int dd = 1; dd < 32; dd <<= 1) {
+                const uint32_t o = __shfl_up_sync(0xffffffffu, inc, dd);
+                if (lane >= dd) inc += o;
+            }
+            tot = __shfl_sync(0xffffffffu, inc, 31);
         }
-        const uint32_t tot = __shfl_sync(0xffffffffu, inc, 31);
         if (cx.cpos + tot > cx.cend) {
             // retire the rest of the slab, reserve a new one (at least the round's candidates)
             for (uint32_t i = cx.cpos + lane; i < cx.cend; i += 32)
@@ -1149,13 +1155,22 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
         const HitRec* seg = a.seg + h0;
         Fx tm{0, 0}, tc{0, 0};
         uint64_t tn = 0;
-        for (uint32_t j = lane; j < L; j += 32) {
-            const HitRec hr = seg[j];
+        auto add_hit = [&](const HitRec& hr) {
             const FxContribution c = fx_contribution(P, hr);
             tm = fx_add(tm, c.mit);
             tc = fx_add(tc, c.cfd);
             tn += c.occ;
+        };
+        // four hits per lane in flight, then the rest one at a time
+        uint32_t j = lane;
+        for (; j + 96 < L; j += 128) {
+            const HitRec h0 = seg[j], h1 = seg[j + 32], h2 = seg[j + 64], h3 = seg[j + 96];
+            add_hit(h0);
+            add_hit(h1);
+            add_hit(h2);
+            add_hit(h3);
         }
+        for (; j < L; j += 32) add_hit(seg[j]);
         tm = fx_warp_sum(tm);
         tc = fx_warp_sum(tc);
         for (int d = 16; d > 0; d >>= 1) tn += __shfl_xor_sync(0xffffffffu, tn, d);
@@ -1979,13 +1994,12 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
                                      BucketStore{ws.bucket_qstart.p, ws.bucket_ustart.p, g0},
                                      nullptr, g1 - g0, ws.scan64.p, &C->bucket_total, st);
         k_units_finalize<<<1, 1, 0, st>>>(C, ws.unit_cap);
-        k_expand_units<<<sms * 8, 256, 0, st>>>(ws.bucket_cnt.p, off, ws.bucket_qstart.p, ws.bucket_ustart.p, g0,
-                                                g1 - g0, ix->n_sites, 1.0 / static_cast<double>(ix->n_sites), cc, C,
-                                                ws.units.p);
-        k_bucket_stats<<<sms * 4, 256, 0, st>>>(ws.bucket_cnt.p, off, g0, g1, ix->d_geom.p, ix->n_sites, C);
+        k_expand_units<<<sms * 8, 256, 0, st>>>(ws.bucket_cnt.p, off, ws.bucket_qstart.p, ws.bucket_ustart.p, g0, g1,
+                                                ix->n_sites, 1.0 / static_cast<double>(ix->n_sites), cc,
+                                                ix->d_geom.p, C, ws.units.p);
         k_probe_scatter<<<pgrid, 256, 0, st>>>(v, R.qsig, wp, ws.probe_gb.p, ws.bucket_cnt.p, ws.bucket_qstart.p,
                                                ws.probe_qr.p);
-        k += 8;
+        k += 7;
         ScanArgs sa;
         sa.rbits = v.rbits;
         sa.rbits_base = v.rbits_base;
