@@ -1212,19 +1212,33 @@ __global__ void __launch_bounds__(256) k_score_sum(ScoreArgs a) {
 }
 
 // Warp per guide whose test fires (at most kWarpSort hits). The reference visits hits by slice,
-// then list position. The hits are first bucketed by slice (counting sort); whole slices are
-// added exactly while the running totals do not fire the test -- within a slice the order then
-// does not matter -- and only the slice where the test fires is sorted by list position (a
-// bitonic network whose comparators all point the same way; missing elements act as +infinity)
-// to find the exact hit where the reference stops. Scores and counts are those at that hit.
+// then list position. The hits are first bucketed by slice (counting sort). Within a slice the
+// order of the additions does not change exact totals, so lane t adds up slice t's hits, and one
+// warp scan over the slice totals gives the running totals at every slice end; the first slice
+// whose end fires the test is the one the reference stops in (the totals only grow, and a slice
+// without hits repeats the test of the slice before it, which did not fire). Only that slice's
+// hits are ordered by list position (a bitonic network whose comparators all point the same way;
+// missing elements act as +infinity) to find the exact hit where the reference stops. Scores and
+// counts are those at that hit. An exit slice with more than kOrdKeys hits goes to the block
+// scorer.
+constexpr int kOrdKeys = 256;
 struct OrderedSmem {
-    uint64_t keys[kWarpSort];
+    uint64_t keys[kOrdKeys];
     uint16_t idx[kWarpSort];
     uint32_t cnt[kMaxSlices + 1];
     uint32_t cur[kMaxSlices];
 };
 
-__global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
+__device__ __forceinline__ uint32_t warp_incl_sum_u32(uint32_t v, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= d) v += o;
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(256, 3) k_score_ordered(ScoreArgs a) {
     extern __shared__ __align__(16) uint8_t s_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     OrderedSmem& W = reinterpret_cast<OrderedSmem*>(s_raw)[warp];
@@ -1245,77 +1259,115 @@ __global__ void __launch_bounds__(256) k_score_ordered(ScoreArgs a) {
         }
         const uint32_t h0 = a.qoff[qi], L = a.qfill[qi];
         const HitRec* seg = a.seg + h0;
-        // counting sort of the hits by slice
+        // counting sort of the hits by slice (four slice reads in flight per lane)
         for (uint32_t t = lane; t <= S; t += 32) W.cnt[t] = 0;
         __syncwarp();
-        for (uint32_t i = lane; i < L; i += 32) atomicAdd(&W.cnt[seg[i].r.y], 1u);
-        __syncwarp();
-        if (lane == 0) {
-            uint32_t acc = 0;
-            for (uint32_t t = 0; t < S; t++) {
-                const uint32_t c = W.cnt[t];
-                W.cnt[t] = acc;
-                W.cur[t] = acc;
-                acc += c;
-            }
-            W.cnt[S] = acc;
+        for (uint32_t i = lane; i < L; i += 128) {
+            uint32_t y[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) y[u] = i + 32 * u < L ? seg[i + 32 * u].r.y : kEmpty;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (y[u] != kEmpty) atomicAdd(&W.cnt[y[u]], 1u);
         }
         __syncwarp();
-        for (uint32_t i = lane; i < L; i += 32) W.idx[atomicAdd(&W.cur[seg[i].r.y], 1u)] = static_cast<uint16_t>(i);
+        uint32_t before = 0;  // hits in the slices of the earlier rounds
+        for (uint32_t t0 = 0; t0 < S; t0 += 32) {
+            const uint32_t t = t0 + lane;
+            const uint32_t v = t < S ? W.cnt[t] : 0u;
+            const uint32_t inc = warp_incl_sum_u32(v, lane);
+            if (t < S) W.cnt[t] = W.cur[t] = before + inc - v;
+            before += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        if (lane == 0) W.cnt[S] = before;
         __syncwarp();
-        // The hits in slice order, 32 at a time, with running exact totals (inclusive warp scans
-        // plus the carry of the earlier chunks). At the last hit of each slice the test is
-        // evaluated on the totals of whole slices; the first slice where it fires is the one the
-        // reference stops in (the totals only grow, so the test fires at every later slice end
-        // too). bm/bc/bn: the totals at the end of the last slice that completed without firing.
+        for (uint32_t i = lane; i < L; i += 128) {
+            uint32_t y[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) y[u] = i + 32 * u < L ? seg[i + 32 * u].r.y : kEmpty;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (y[u] != kEmpty) W.idx[atomicAdd(&W.cur[y[u]], 1u)] = static_cast<uint16_t>(i + 32 * u);
+        }
+        __syncwarp();
+        // running totals at the slice ends, 32 slices per round; bm/bc/bn: the totals before the
+        // exit slice
         Fx cm = rm, cc = rc, bm = rm, bc = rc;
         uint64_t cn = rn, bn = rn;
         int exit_sl = -1;
-        for (uint32_t c0 = 0; c0 < L && exit_sl < 0; c0 += 32) {
-            const uint32_t t = c0 + lane;
-            FxContribution c{{0, 0}, {0, 0}, 0};
-            uint32_t sl = 0xFFFFFFFFu;
-            if (t < L) {
-                const HitRec hr = seg[W.idx[t]];
-                sl = hr.r.y;
-                c = fx_contribution(P, hr);
+        for (uint32_t t0 = 0; t0 < S && exit_sl < 0; t0 += 32) {
+            const uint32_t t = t0 + lane;
+            // slice t's exact totals (four hits in flight)
+            Fx sm{0, 0}, sc{0, 0};
+            uint64_t so = 0;
+            if (t < S) {
+                const uint32_t j1 = W.cnt[t + 1];
+                for (uint32_t j = W.cnt[t]; j < j1; j += 4) {
+                    double hm[4], hc[4];
+                    uint32_t ho[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+                        if (j + u < j1) {
+                            const HitRec* hp = seg + W.idx[j + u];
+                            hm[u] = hp->mit;
+                            hc[u] = hp->cfd;
+                            ho[u] = hp->r.w;
+                        }
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+                        if (j + u < j1) {
+                            sm = fx_add(sm, fx_from(P.calc_mit ? hm[u] : 0.0));
+                            sc = fx_add(sc, fx_from(P.calc_cfd ? hc[u] : 0.0));
+                            so += ho[u];
+                        }
+                }
             }
-            uint32_t nsl = __shfl_down_sync(0xffffffffu, sl, 1);
-            if (lane == 31) nsl = t + 1 < L ? seg[W.idx[t + 1]].r.y : 0xFFFFFFFFu;
-            const bool end = t < L && nsl != sl;
-            const Fx im = fx_add(fx_warp_incl(c.mit, lane), cm);
-            const Fx ic = fx_add(fx_warp_incl(c.cfd, lane), cc);
-            const uint64_t in = warp_incl_sum_u64(c.occ, lane) + cn;
-            const bool fire = end && exit_test(P, fx_double(im), fx_double(ic));
-            const unsigned ends = __ballot_sync(0xffffffffu, end), fires = __ballot_sync(0xffffffffu, fire);
-            const unsigned done = fires ? ends & ((1u << (__ffs(fires) - 1)) - 1u) : ends;  // ends before the first fire
-            if (done) {
-                const int e = 31 - __clz(done);
-                bm = Fx{__shfl_sync(0xffffffffu, im.hi, e), __shfl_sync(0xffffffffu, im.lo, e)};
-                bc = Fx{__shfl_sync(0xffffffffu, ic.hi, e), __shfl_sync(0xffffffffu, ic.lo, e)};
-                bn = __shfl_sync(0xffffffffu, in, e);
+            const Fx im = fx_add(fx_warp_incl(sm, lane), cm);
+            const Fx ic = fx_add(fx_warp_incl(sc, lane), cc);
+            const uint64_t in = warp_incl_sum_u64(so, lane) + cn;
+            const unsigned fires = __ballot_sync(0xffffffffu, t < S && exit_test(P, fx_double(im), fx_double(ic)));
+            if (fires) {
+                const int f = __ffs(fires) - 1, pl = f > 0 ? f - 1 : 0;
+                const Fx pm{__shfl_sync(0xffffffffu, im.hi, pl), __shfl_sync(0xffffffffu, im.lo, pl)};
+                const Fx pc{__shfl_sync(0xffffffffu, ic.hi, pl), __shfl_sync(0xffffffffu, ic.lo, pl)};
+                const uint64_t pn = __shfl_sync(0xffffffffu, in, pl);
+                exit_sl = static_cast<int>(t0) + f;
+                bm = f > 0 ? pm : cm;
+                bc = f > 0 ? pc : cc;
+                bn = f > 0 ? pn : cn;
             }
-            if (fires) exit_sl = static_cast<int>(__shfl_sync(0xffffffffu, sl, __ffs(fires) - 1));
             cm = Fx{__shfl_sync(0xffffffffu, im.hi, 31), __shfl_sync(0xffffffffu, im.lo, 31)};
             cc = Fx{__shfl_sync(0xffffffffu, ic.hi, 31), __shfl_sync(0xffffffffu, ic.lo, 31)};
             cn = __shfl_sync(0xffffffffu, in, 31);
         }
-        if (exit_sl < 0) {
+        // the exit slice's hits as (list position, hit) keys
+        const uint32_t b0 = exit_sl >= 0 ? W.cnt[exit_sl] : 0u;
+        const uint32_t ns = exit_sl >= 0 ? W.cnt[exit_sl + 1] - b0 : 0u;
+        if (ns <= static_cast<uint32_t>(kOrdKeys))
+            for (uint32_t j = lane; j < ns; j += 32) {
+                const uint32_t i = W.idx[b0 + j];
+                W.keys[j] = (static_cast<uint64_t>(seg[i].r.x) << 10) | i;
+            }
+        if (ns == 0) {
             // no slice end fires (k_score_sum fired on the same exact totals, so this does not
             // happen): the one-by-one rescoring settles it
             if (lane == 0) a.replay[atomicAdd(&a.counters->n_replay, 1u)] = static_cast<uint32_t>(qi);
             __syncwarp();
             continue;
         }
-        const uint32_t b0 = W.cnt[exit_sl], ns = W.cnt[exit_sl + 1] - b0;
+        if (ns > static_cast<uint32_t>(kOrdKeys)) {
+            // more hits in the exit slice than the warp orders: the block scorer takes the guide
+            if (lane == 0) a.big[atomicAdd(&a.counters->n_big, 1u)] = static_cast<uint32_t>(qi);
+            __syncwarp();
+            continue;
+        }
         rm = bm;
         rc = bc;
         rn = bn;
         // the test fires inside this slice: order its hits by list position
         uint32_t P2 = 1;
         while (P2 < ns) P2 <<= 1;
-        for (uint32_t j = lane; j < P2; j += 32)
-            W.keys[j] = j < ns ? (static_cast<uint64_t>(seg[W.idx[b0 + j]].r.x) << 10) | W.idx[b0 + j] : ~0ull;
+        for (uint32_t j = ns + lane; j < P2; j += 32) W.keys[j] = ~0ull;
         __syncwarp();
         for (uint32_t k = 2; k <= P2; k <<= 1) {
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
@@ -1592,11 +1644,25 @@ __global__ void __launch_bounds__(256) k_replay(ScoreArgs a, IndexView v) {
     }
 }
 
+// Distinct sites: the population count of the site bitmap (16-byte reads, four in flight per
+// thread; the allocation is 256-byte aligned, the last words < 4 are read one at a time).
 __global__ void k_popcount(const uint32_t* __restrict__ bm, uint64_t words, Counters* c) {
     uint64_t acc = 0;
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < words;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        acc += __popc(bm[i]);
+    const uint4* v = reinterpret_cast<const uint4*>(bm);
+    const uint64_t nv = words / 4, T = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    for (; i + 3 * T < nv; i += 4 * T) {
+        const uint4 a = v[i], b = v[i + T], d = v[i + 2 * T], e = v[i + 3 * T];
+        acc += __popc(a.x) + __popc(a.y) + __popc(a.z) + __popc(a.w) + __popc(b.x) + __popc(b.y) + __popc(b.z) +
+               __popc(b.w) + __popc(d.x) + __popc(d.y) + __popc(d.z) + __popc(d.w) + __popc(e.x) + __popc(e.y) +
+               __popc(e.z) + __popc(e.w);
+    }
+    for (; i < nv; i += T) {
+        const uint4 a = v[i];
+        acc += __popc(a.x) + __popc(a.y) + __popc(a.z) + __popc(a.w);
+    }
+    const uint64_t t = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (t < words - nv * 4) acc += __popc(bm[nv * 4 + t]);
     for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
     if ((threadIdx.x & 31) == 0 && acc) atomicAdd(reinterpret_cast<unsigned long long*>(&c->distinct), acc);
 }
@@ -2059,7 +2125,7 @@ uint64_t enqueue_pipeline(issl_index* ix, Workspace& ws, const RunSpec& R, cudaS
         a.first_wave = first;
         a.last_wave = last;
         k_score_sum<<<grid_for(n, 8, sms * 8), 256, 0, st>>>(a);
-        k_score_ordered<<<sms * 4, 256, 8 * sizeof(OrderedSmem), st>>>(a);
+        k_score_ordered<<<sms * 3, 256, 8 * sizeof(OrderedSmem), st>>>(a);
         k_score_block<<<sms * 2, 256, kBlockHits * sizeof(uint64_t), st>>>(a);
         k += 3;
         if (last) {
