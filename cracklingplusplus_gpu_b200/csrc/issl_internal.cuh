@@ -180,7 +180,7 @@ struct issl_index {
     std::unique_ptr<issl::Workspace> ws;
     issl_score_stats stats{};
     // scan unit size per bucket-size class, staging depth, blocks per SM, first slice wave
-    issl_tuning tuning{{1024, 1024, 1024}, 3, 0, 1};
+    issl_tuning tuning{{1024, 1024, 1024}, 2, 0, 1};
     uint32_t tuning_version = 0;
     issl::IndexView view() const;
     issl_index();  // defined where Workspace is complete

@@ -880,7 +880,7 @@ __device__ __forceinline__ Contribution contribution(const Tables& T, const Scor
 // MIT and CFD contributions are computed here, where the reads leave the arithmetic units idle, and
 // its record is written to the next free slot of its guide's segment, so the scorers read only
 // contiguous data.
-__global__ void __launch_bounds__(256, 5)
+__global__ void __launch_bounds__(256, 8)
     k_cand_resolve(const uint2* __restrict__ cands, Counters* c, IndexView ix, const uint64_t* __restrict__ qsig,
                    const uint32_t* __restrict__ qoff, uint32_t* __restrict__ qfill, const Tables* __restrict__ tables,
                    HitRec* __restrict__ seg, const SetDesc* __restrict__ sets, const uint16_t* __restrict__ qset) {
@@ -901,9 +901,11 @@ __global__ void __launch_bounds__(256, 5)
     both.calc_cfd = 1;
     const uint32_t n = c->n_cand;
     uint32_t owned_here = 0;
-    // two candidates per thread and round, their reads issued together (the random list-entry
-    // reads are the bound: more of them in flight per thread; four gave no further gain)
-    constexpr int U = 2;
+    // one candidate per thread and round, eight blocks per SM (the grid is one wave): at the
+    // 300M-site workload two or four candidates per thread with five or four blocks were 4-6%
+    // slower (random list-entry reads, the L2 atomics of the segment fill and the hit writes
+    // are all latency-bound)
+    constexpr int U = 1;
     const uint32_t T = gridDim.x * blockDim.x;
     for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * T) {
         uint2 r[U];

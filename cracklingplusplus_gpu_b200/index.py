@@ -175,7 +175,7 @@ class Index:
         check(lib().issl_get_tuning(self._h, C.byref(out)))
         return out
 
-    def set_tuning(self, chunk=(1024, 1024, 1024), stages: int = 3, blocks_per_sm: int = 0,
+    def set_tuning(self, chunk=(1024, 1024, 1024), stages: int = 2, blocks_per_sm: int = 0,
                    first_wave: int = 1) -> None:
         t = Tuning((C.c_uint32 * 3)(*chunk), stages, blocks_per_sm, first_wave)
         check(lib().issl_set_tuning(self._h, C.byref(t)))

@@ -212,7 +212,7 @@ int issl_last_stats(const issl_index* index, issl_score_stats* out);
  * speed and memory do. */
 typedef struct {
     uint32_t chunk[3];       /* buckets of < 64, 64..4095, >= 4096 entries: 256, 512 or 1024 */
-    uint32_t stages;         /* 2..4 (default 3) */
+    uint32_t stages;         /* 2..4 (default 2: seven scan blocks fit an SM) */
     uint32_t blocks_per_sm;  /* 0 = as many as fit (default) */
     uint32_t first_wave;     /* slices scored before the rest (default 1; 0 = all in one wave):
                                 guides whose early exit fires there never probe the later slices */

@@ -184,7 +184,7 @@ def test_invalid_tuning_rejected(native, c2):
                 ((1024, 1024, 1024), 3, 0, 65)]:
         with pytest.raises(native.IsslError):
             ix.set_tuning(*bad)
-    assert ix.get_tuning().as_tuple() == ((1024, 1024, 1024), 3, 0, 1)
+    assert ix.get_tuning().as_tuple() == ((1024, 1024, 1024), 2, 0, 1)  # the default is kept
 
 
 def test_autotune_and_cache(native, c2, tmp_path):
