@@ -1107,7 +1107,9 @@ def bench_served(args, pkg, ix, q, base):
             r = srv.wait(t)
             replies.append((k, r.info.latency_ms, r.info.queue_ms, r.info.batch_requests, req, r.result))
 
-    cols = [threading.Thread(target=collector) for _ in range(4)]
+    # daemon collectors, stopped in any case: an error in the submission loop must not leave the
+    # process waiting for them at exit
+    cols = [threading.Thread(target=collector, daemon=True) for _ in range(4)]
     for c in cols:
         c.start()
     start = time.perf_counter()
@@ -1115,21 +1117,23 @@ def bench_served(args, pkg, ix, q, base):
     n_req = offered = 0
     sample_reqs = []
     arrivals = []  # (arrival time, request): the same request set for the plain form below
-    while True:
-        next_t += rng.exponential(1.0 / rate)
-        if next_t - start > seconds:
-            break
-        delay = next_t - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        req = draw()
-        t = srv.submit(*req)
-        n_req += 1
-        offered += len(req[0])
-        arrivals.append((time.perf_counter() - start, req))
-        tickets.put((t, len(req[0]), req if len(sample_reqs) < 40 and n_req % 25 == 0 else None))
-    for _ in cols:
-        tickets.put(None)
+    try:
+        while True:
+            next_t += rng.exponential(1.0 / rate)
+            if next_t - start > seconds:
+                break
+            delay = next_t - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            req = draw()
+            t = srv.submit(*req)
+            n_req += 1
+            offered += len(req[0])
+            arrivals.append((time.perf_counter() - start, req))
+            tickets.put((t, len(req[0]), req if len(sample_reqs) < 40 and n_req % 25 == 0 else None))
+    finally:
+        for _ in cols:
+            tickets.put(None)
     for c in cols:
         c.join()
     wall = time.perf_counter() - start

@@ -7,7 +7,8 @@
 // footprint stays within the slot's share of the free device memory; the batch is scored as one
 // pass (each request is one guide set with its own method / threshold / mismatch bound). Other
 // slots keep taking requests meanwhile, so requests that arrive while batches are on the GPU
-// are admitted as soon as a slot frees up, and the batches overlap on the device.
+// are admitted as soon as a slot frees up, and the batches overlap on the device. A request too
+// large for one batch (guide limit or footprint) is queued as consecutive parts of equal size.
 //
 // This file has no GPU code: the executor that scores a batch is a template parameter, so the
 // same scheduler runs in the library (a GPU executor) and in host-only tests (a fake one).
@@ -56,6 +57,14 @@ struct Footprint {
         return fixed + n * per_guide + static_cast<uint64_t>(static_cast<double>(n) * candidates_per_guide) *
                                            per_candidate;
     }
+    // the most guides whose footprint stays within `budget` (0 if not even one fits)
+    uint64_t guides_within(uint64_t budget) const {
+        if (budget < bytes(1)) return 0;
+        const double per = static_cast<double>(per_guide) + candidates_per_guide * static_cast<double>(per_candidate);
+        uint64_t m = static_cast<uint64_t>(static_cast<double>(budget - fixed) / per);
+        while (m > 1 && bytes(m) > budget) m--;
+        return m ? m : 1;
+    }
 };
 
 struct Request {
@@ -73,6 +82,12 @@ struct Request {
     int status = ISSL_OK;
     std::string error;
     bool done = false;
+    // a request larger than one batch may hold is scored as consecutive parts: each part is a
+    // request of its own in the queue, `parent` the caller's request, which completes with its last
+    Request* parent = nullptr;
+    uint64_t part_off = 0;  // first guide of the part within the parent
+    uint32_t parts_left = 0;
+    std::vector<std::unique_ptr<Request>> parts;
 };
 
 struct Stats {
@@ -106,17 +121,16 @@ public:
     Scheduler(const Scheduler&) = delete;
     Scheduler& operator=(const Scheduler&) = delete;
 
+    // A request above the batch limit, or whose modelled footprint exceeds a slot's share of the
+    // device memory, is scored as consecutive parts of equal size (guides are independent); only
+    // a request of which not even one guide fits a slot is refused (ISSL_ERR_BUSY).
     int submit(std::unique_ptr<Request> r, uint64_t* ticket, std::string* err) {
         const uint64_t n = r->sigs.size();
         std::lock_guard<std::mutex> lk(mu_);
-        if (n > cfg_.max_batch_guides) {
-            *err = "request larger than the server's batch limit (" + std::to_string(cfg_.max_batch_guides) +
-                   " guides); split it";
-            return ISSL_ERR_ARG;
-        }
-        if (fp_.bytes(n) > cfg_.slot_budget_bytes) {
-            *err = "request needs more device memory than a slot may use (" + std::to_string(fp_.bytes(n)) +
-                   " > " + std::to_string(cfg_.slot_budget_bytes) + " bytes)";
+        const uint64_t fit = std::min<uint64_t>(cfg_.max_batch_guides, fp_.guides_within(cfg_.slot_budget_bytes));
+        if (n && fit == 0) {
+            *err = "request needs more device memory than a slot may use (" + std::to_string(fp_.bytes(1)) +
+                   " > " + std::to_string(cfg_.slot_budget_bytes) + " bytes for one guide)";
             return ISSL_ERR_BUSY;
         }
         r->ticket = ++next_ticket_;
@@ -130,7 +144,29 @@ public:
             done_cv_.notify_all();
             return ISSL_OK;
         }
-        pending_.push_back(p);
+        if (n <= fit) {
+            pending_.push_back(p);
+        } else {
+            const uint64_t k = (n + fit - 1) / fit, m = (n + k - 1) / k;
+            p->mit.resize(n);
+            p->cfd.resize(n);
+            p->code.resize(n);
+            p->count.resize(n);
+            p->parts_left = static_cast<uint32_t>(k);
+            for (uint64_t off = 0; off < n; off += m) {
+                auto part = std::make_unique<Request>();
+                part->sigs.assign(p->sigs.begin() + off, p->sigs.begin() + std::min(n, off + m));
+                part->method = p->method;
+                part->max_dist = p->max_dist;
+                part->threshold = p->threshold;
+                part->ticket = p->ticket;
+                part->t_submit = p->t_submit;
+                part->parent = p;
+                part->part_off = off;
+                pending_.push_back(part.get());
+                p->parts.push_back(std::move(part));
+            }
+        }
         pending_guides_ += n;
         work_cv_.notify_one();
         return ISSL_OK;
@@ -253,8 +289,34 @@ private:
                 r->status = st;
                 r->error = err;
                 r->done = true;
-                latencies_.push_back(ms_between(r->t_submit, t_done));
                 guides_done_ += r->sigs.size();
+                Request* q = r->parent;
+                if (!q) {
+                    latencies_.push_back(ms_between(r->t_submit, t_done));
+                    continue;
+                }
+                // a part: its results go to the caller's request, which is done with its last part
+                if (st == ISSL_OK) {
+                    std::copy(r->mit.begin(), r->mit.end(), q->mit.begin() + r->part_off);
+                    std::copy(r->cfd.begin(), r->cfd.end(), q->cfd.begin() + r->part_off);
+                    std::copy(r->code.begin(), r->code.end(), q->code.begin() + r->part_off);
+                    std::copy(r->count.begin(), r->count.end(), q->count.begin() + r->part_off);
+                } else if (q->status == ISSL_OK) {
+                    q->status = st;
+                    q->error = err;
+                }
+                std::vector<double>().swap(r->mit);
+                std::vector<double>().swap(r->cfd);
+                if (q->parts_left == static_cast<uint32_t>(q->parts.size()) || r->t_admit < q->t_admit)
+                    q->t_admit = r->t_admit;  // the first part's admission
+                q->batch_guides = std::max(q->batch_guides, r->batch_guides);
+                q->batch_requests = std::max(q->batch_requests, r->batch_requests);
+                q->slot = r->slot;
+                if (--q->parts_left == 0) {
+                    q->t_done = t_done;
+                    q->done = true;
+                    latencies_.push_back(ms_between(q->t_submit, t_done));
+                }
             }
             lk.unlock();
             done_cv_.notify_all();

@@ -287,7 +287,7 @@ int issl_batch_stats(const issl_batch* batch, issl_score_stats* out);
 typedef struct {
     uint32_t n_slots;           /* batches on the GPU at once (0 = 3) */
     uint32_t max_wait_us;       /* a free slot waits this long for more arrivals before scoring (0) */
-    uint64_t max_batch_guides;  /* guides per batch, and per request at most (0 = 131072) */
+    uint64_t max_batch_guides;  /* guides per batch (0 = 131072); larger requests run in parts */
     uint64_t headroom_bytes;    /* device memory left free beside the index and the slots (0 = 16 GiB) */
 } issl_server_config;
 
@@ -315,8 +315,9 @@ typedef struct issl_server issl_server;
 int issl_server_create(issl_index* index, const issl_server_config* config, issl_server** out);
 
 /* Queues n guides (host memory, packed signatures; copied) as one request and returns its ticket
- * at once. ISSL_ERR_ARG for a bad method / max_dist or n above max_batch_guides, ISSL_ERR_BUSY when
- * the request alone needs more device memory than a slot may use. */
+ * at once. A request above max_batch_guides, or whose modelled device footprint exceeds a slot's
+ * share, is scored as consecutive parts (its ticket completes with the last one). ISSL_ERR_ARG
+ * for a bad method / max_dist, ISSL_ERR_BUSY when not even one guide fits a slot. */
 int issl_server_submit(issl_server* server, const uint64_t* sigs, size_t n, int method, double threshold,
                        int max_dist, uint64_t* ticket);
 

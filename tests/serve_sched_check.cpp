@@ -1,7 +1,8 @@
 // Host-only checks of the scoring server's scheduler (cracklingplusplus_gpu_b200/csrc/serve_sched.hpp)
 // with a fake executor: results reach the right requests, batching and overlap happen, batches
 // respect the guide limit and the slot's memory budget, admission is in arrival order, the
-// footprint estimate grows with what batches used, waits time out, and shutdown drains the queue.
+// footprint estimate grows with what batches used, requests too large for one batch are scored in
+// parts, waits time out, and shutdown drains the queue.
 // Prints "ok" and exits 0 when every check holds.
 #include <atomic>
 #include <cstdio>
@@ -151,8 +152,20 @@ int main() {
         Scheduler<FakeExec> s(cfg, fp, ex);
         uint64_t ticket;
         std::string err;
-        CHECK(s.submit(make(1, 600, 2, 75, 4), &ticket, &err) == ISSL_ERR_BUSY);   // needs more than a slot
-        CHECK(s.submit(make(1, 1001, 2, 75, 4), &ticket, &err) == ISSL_ERR_ARG);   // above the batch limit
+        {  // needs more than a slot's memory (600 > 500 guides) and exceeds the batch limit (1001 > 1000):
+           // both are scored in parts of at most 500 guides, with every guide's result in place
+            uint64_t t1, t2;
+            CHECK(s.submit(make(1, 600, 2, 75, 4), &t1, &err) == ISSL_OK);
+            CHECK(s.submit(make(2, 1001, 1, 60, 3), &t2, &err) == ISSL_OK);
+            std::unique_ptr<Request> r1, r2;
+            CHECK(s.wait(t1, -1, &r1, &err) == ISSL_OK && r1->sigs.size() == 600 && r1->parts.size() == 2);
+            CHECK(s.wait(t2, -1, &r2, &err) == ISSL_OK && r2->sigs.size() == 1001 && r2->parts.size() == 3);
+            check_results(*r1, 1);
+            check_results(*r2, 2);
+            CHECK(r1->t_submit <= r1->t_admit && r1->t_admit <= r1->t_done);
+            CHECK(ex.max_batch <= 500);
+            ex.admitted.clear();
+        }
         std::vector<uint64_t> tickets;
         for (int k = 0; k < 12; k++) {
             CHECK(s.submit(make(100 + k, 200, 2, 75, 4), &ticket, &err) == ISSL_OK);
@@ -166,14 +179,33 @@ int main() {
         }
         CHECK(ex.max_batch <= 500);
         for (size_t k = 1; k < ex.admitted.size(); k++) CHECK(ex.admitted[k] > ex.admitted[k - 1]);  // FIFO
-        // a batch that used many candidates raises the estimate: 400 guides no longer fit
+        // a batch that used many candidates raises the estimate: 400 guides no longer fit one batch
+        // and run in parts
         ex.cand_per_guide = 8;
         CHECK(s.submit(make(7, 100, 2, 75, 4), &ticket, &err) == ISSL_OK);
         std::unique_ptr<Request> r;
         CHECK(s.wait(ticket, -1, &r, &err) == ISSL_OK);
-        CHECK(s.submit(make(8, 400, 2, 75, 4), &ticket, &err) == ISSL_ERR_BUSY);
+        ex.max_batch = 0;
+        CHECK(s.submit(make(8, 400, 2, 75, 4), &ticket, &err) == ISSL_OK);
+        CHECK(s.wait(ticket, -1, &r, &err) == ISSL_OK && r->parts.size() >= 2);
+        check_results(*r, 8);
+        CHECK(ex.max_batch < 400);
         CHECK(s.submit(make(9, 0, 2, 75, 4), &ticket, &err) == ISSL_OK);  // empty request completes at once
         CHECK(s.wait(ticket, 0, &r, &err) == ISSL_OK && r->sigs.empty());
+        CHECK(s.stats(false).requests == 16);  // a request scored in parts counts once
+    }
+    {  // refused only when not even one guide fits a slot
+        FakeExec ex;
+        Config cfg;
+        cfg.n_slots = 1;
+        Footprint fp;
+        fp.fixed = 1000;
+        fp.per_guide = 100;
+        cfg.slot_budget_bytes = 1050;
+        Scheduler<FakeExec> s(cfg, fp, ex);
+        uint64_t ticket;
+        std::string err;
+        CHECK(s.submit(make(1, 3, 2, 75, 4), &ticket, &err) == ISSL_ERR_BUSY);
     }
     {  // timeouts and draining on shutdown
         FakeExec ex;

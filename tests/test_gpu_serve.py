@@ -81,8 +81,14 @@ def test_server_limits(native, c2):
     z, _, ix = c2
     q = np.resize(z["queries"], 1001)  # the case's guides, repeated
     with native.Server(ix, n_slots=2, max_batch_guides=1000) as srv:
-        with pytest.raises(native.IsslError):
-            srv.submit(q[:1001], "and", 75.0)  # above the batch limit
+        # above the batch limit: scored in parts, each guide's result as if scored alone
+        t = srv.submit(q[:1001], "and", 75.0)
+        rep = srv.wait(t)
+        alone = ix.score(q[:1001], "and", 75.0, distinct=False)
+        assert rep.result.code == alone.code
+        assert np.array_equal(rep.result.mit, alone.mit) and np.array_equal(rep.result.cfd, alone.cfd)
+        assert np.array_equal(rep.result.count, alone.count)
+        assert rep.info.batch_guides <= 1000
         with pytest.raises(native.IsslError):
             srv.submit(q[:10], 9, 75.0)         # no such method
         t = srv.submit(q[:0], "and", 75.0)
