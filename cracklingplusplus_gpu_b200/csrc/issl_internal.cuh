@@ -234,6 +234,12 @@ void radix_sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, ui
 // device bytes of a scoring workspace: fixed + n * per_guide + candidates * per_candidate (score.cu)
 void workspace_model(const issl_index* ix, uint64_t* fixed, uint64_t* per_guide, uint64_t* per_candidate);
 
+// Sizes a batch context's workspace, from its next call on, for batches of up to `guides` guides
+// and as many candidate slots as `budget_bytes` leaves room for, so that serving never grows (and
+// reallocates, which synchronises the device) while other batches run (score.cu). Dropped again
+// if the device cannot hold it.
+void batch_set_capacity_floor(issl_batch* batch, uint64_t guides, uint64_t budget_bytes);
+
 // tables (tables.cpp)
 const std::vector<double>& mit_rank_table();   // 6195 entries indexed by subset rank
 const double* cfd_pos_table();

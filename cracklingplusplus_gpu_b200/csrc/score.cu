@@ -210,6 +210,7 @@ struct issl::Workspace {
     uint64_t staged = 0;    // host-list index: bytes the last pipeline copies from host memory
     uint32_t tuning_version = ~0u;  // version of the index's tuning the scan is configured for
     double cand_density = 64.0;     // candidate slots per guide recent runs needed (largest wave)
+    uint64_t q_floor = 0, cand_floor = 0;  // capacities held whatever a call needs (server slots)
     double cand_seen = 0.0, guides_seen = 0.0;  // their decayed, size-weighted sums
     uint64_t epoch = 0;             // bumped whenever a buffer is reallocated
     // batch form: set table (header + sets) on the device and its pinned host staging, the
@@ -1829,11 +1830,19 @@ void window_capacity(const issl_index* ix, uint64_t* id_words, uint64_t* code_wo
 void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st);
 
 void ensure_capacity(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st) {
-    with_alloc_guard(ws, [&] { ensure_capacity_impl(ix, ws, n, batch, st); });
+    try {
+        with_alloc_guard(ws, [&] { ensure_capacity_impl(ix, ws, n, batch, st); });
+    } catch (const Error& e) {
+        // a capacity floor the device cannot hold is dropped; the call then sizes for itself
+        if (e.code != ISSL_ERR_NOMEM || (!ws.q_floor && !ws.cand_floor)) throw;
+        ws.q_floor = ws.cand_floor = 0;
+        with_alloc_guard(ws, [&] { ensure_capacity_impl(ix, ws, n, batch, st); });
+    }
 }
 
 void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, cudaStream_t st) {
     const uint64_t S = ix->n_slices, G = ix->n_buckets;
+    n = std::max<size_t>(n, ws.q_floor);
     apply_tuning(ix, ws);
     if (ix->host_lists) {
         if (!ws.copy_stream) {
@@ -1908,7 +1917,7 @@ void ensure_capacity_impl(issl_index* ix, Workspace& ws, size_t n, bool batch, c
     // device, which stalls concurrent work); grown on demand after an overflow
     size_t want_cands = static_cast<size_t>(static_cast<double>(n) * ws.cand_density * 1.1) + 65536 +
                         static_cast<size_t>(ws.scan_blocks) * kScanWarps * kCandSlab;
-    want_cands = std::min(want_cands, kMaxCandSlots);
+    want_cands = std::min(std::max<size_t>(want_cands, ws.cand_floor), kMaxCandSlots);
     if (ws.cand_cap < want_cands) {
         want_cands = std::min(std::max<size_t>(want_cands, ws.cand_cap + ws.cand_cap / 2), kMaxCandSlots);
         ws.cands.reserve(want_cands);
@@ -2382,6 +2391,16 @@ struct issl_batch {
         if (ev1) cudaEventDestroy(ev1);
     }
 };
+
+void issl::batch_set_capacity_floor(issl_batch* b, uint64_t guides, uint64_t budget_bytes) {
+    uint64_t fixed = 0, per_guide = 0, per_cand = 0;
+    workspace_model(b->ix, &fixed, &per_guide, &per_cand);
+    const uint64_t used = fixed + guides * per_guide;
+    b->ws->q_floor = guides;
+    // at most 4096 candidates per guide: a small server on a large device does not take it all
+    const uint64_t room = budget_bytes > used ? (budget_bytes - used) / per_cand : 0;
+    b->ws->cand_floor = std::min<uint64_t>({room, guides * 4096, kMaxCandSlots});
+}
 
 namespace issl {
 namespace {

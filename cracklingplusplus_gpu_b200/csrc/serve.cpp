@@ -116,6 +116,8 @@ int issl_server_create(issl_index* ix, const issl_server_config* config, issl_se
         const uint64_t cap = cfg.max_batch_guides;
         for (auto& s : srv->exec.slots) {
             if (issl_batch_create(ix, &s.batch) != ISSL_OK) throw issl::Error(ISSL_ERR_CUDA, issl_last_error());
+            // the slot's workspace takes its whole share at its first batch and keeps it
+            issl::batch_set_capacity_floor(s.batch, cap, cfg.slot_budget_bytes);
             ISSL_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&s.sigs), cap * 8, cudaHostAllocDefault));
             ISSL_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&s.mit), cap * 8, cudaHostAllocDefault));
             ISSL_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&s.cfd), cap * 8, cudaHostAllocDefault));
