@@ -152,8 +152,9 @@ int issl_score_device(issl_index* index, const uint64_t* d_sigs, size_t n, int m
  * Same arguments and results as issl_score_device (minus the distinct count), buffers in device
  * memory of the index's device, enqueued on `stream` (NULL = the default stream); the call waits
  * for the kernel to finish, then reads the overflow flag. Each guide's sums are accumulated one
- * addition at a time in the reference's order, as the reference does. Limits: at most ISSL_STATIC_MAX_GUIDES guides per call (larger n is
- * rejected with ISSL_ERR_ARG) and at most ISSL_STATIC_MAX_HITS owned off-target hits per guide
+ * addition at a time in the reference's order, as the reference does. Limits: at most
+ * ISSL_STATIC_MAX_GUIDES guides per call (larger n is rejected with ISSL_ERR_ARG) and at most
+ * ISSL_STATIC_MAX_HITS owned off-target hits per guide
  * (a guide beyond that makes the call fail with ISSL_ERR_UNSUPPORTED; its outputs are not set).
  * The first call on a device looks up the scratch address and uploads the penalty tables; make
  * that first call before any stream capture. Every call shares the one scratch array, so calls
